@@ -1,0 +1,526 @@
+// Right-preconditioned BiCGSTAB (the recurrences of cublas2_pbicgstabv2,
+// include/bicgstab/bicgstab_solver.h:33-275) as five fused kernels per
+// iteration, all scalars resident on the device, one CUDA graph per chunk of
+// iterations:
+//
+//   K1 k_bi_py     p = r + beta (p - omega ay) (computed on the fly at every
+//                  gathered column, own row stored), y = M p
+//   K2 k_bi_ay     ay = A y, (r*, ay)                 -> alpha = rho / (r*, ay)
+//   K3 k_bi_sz     s = r - alpha ay (on the fly, own row stored), z = M s
+//   K4 k_bi_az     az = A z, (az, s), (az, az)         -> omega
+//   K5 k_bi_xr     x += alpha y + omega z, r = s - omega az, (r*, r), (r, r)
+//                                                     -> rho, beta, ||r||, stop test
+//
+// The reference issues 4 SpMV + 12 BLAS-1 calls and 5 blocking host reads per
+// iteration (bicgstab_solver.h:138-232).  Reductions end in the last block to
+// arrive (per-block partials summed in block order), so every dot product is
+// deterministic for a given grid.
+//
+// Precision forms (template VT / MT / IT):
+//   FP64   p, y, z, r* double; M double; int32 column indices
+//   mixed  p, y, z, r* float; M float or bf16; int16 column deltas when
+//          every |col - row| < 32768.  A, x, r, s, ay, az, every dot product and
+//          the rho/alpha/omega/beta recurrences stay FP64.  x and r are updated
+//          with exactly the y, z, A y, A z that were stored, so the recurrence
+//          residual tracks b - A x to FP64 rounding.
+#include <cmath>
+
+#include "internal.cuh"
+
+namespace dcu {
+namespace {
+
+constexpr int BI_BLOCK = 256;
+constexpr int BI_WARPS = BI_BLOCK / 32;
+constexpr int CHUNK_ITERS = 8;  // iterations per graph launch
+
+enum { ST_RUN = -1 };
+
+struct Scal {
+  double rho, alpha, omega, beta, res, thr, bnorm, true_res;
+  int it, done, status, pidx;
+  int verify, verify_pending, maxiter, replacements;
+  unsigned counter[8];
+};
+
+// ---- loads -----------------------------------------------------------------
+__device__ __forceinline__ double ldm(const double* p) { return __ldcs(p); }
+__device__ __forceinline__ double ldm(const float* p) { return (double)__ldcs(p); }
+__device__ __forceinline__ double ldm(const __nv_bfloat16* p) {
+  const unsigned short u = __ldcs(reinterpret_cast<const unsigned short*>(p));
+  return (double)__uint_as_float((unsigned)u << 16);
+}
+__device__ __forceinline__ int ldcol(const int* ix, long long q, int) { return __ldcs(ix + q); }
+__device__ __forceinline__ int ldcol(const int16_t* ix, long long q, int r) { return r + (int)__ldcs(ix + q); }
+
+template <typename T>
+__device__ __forceinline__ double ldv(const T* p) { return (double)__ldg(p); }
+
+// One SELL-32 row: sum_k val[q] * xf(col[q]).  A warp covers one slice, so
+// each k step reads 32 consecutive slots.
+template <typename MT, typename IT, typename F>
+__device__ __forceinline__ double sell_row(const long long* __restrict__ off, const MT* __restrict__ val,
+                                           const IT* __restrict__ ix, int r, F xf) {
+  const int s = r >> 5;
+  const long long o0 = __ldg(off + s), o1 = __ldg(off + s + 1);
+  const long long base = o0 + (r & 31);
+  const int w = (int)((o1 - o0) >> 5);
+  double acc = 0.0;
+  int k = 0;
+  for (; k + 4 <= w; k += 4) {
+    const long long q = base + 32ll * k;
+    const double a0 = ldm(val + q), a1 = ldm(val + q + 32), a2 = ldm(val + q + 64), a3 = ldm(val + q + 96);
+    const int c0 = ldcol(ix, q, r), c1 = ldcol(ix, q + 32, r), c2 = ldcol(ix, q + 64, r), c3 = ldcol(ix, q + 96, r);
+    acc += a0 * xf(c0);
+    acc += a1 * xf(c1);
+    acc += a2 * xf(c2);
+    acc += a3 * xf(c3);
+  }
+  for (; k < w; ++k) {
+    const long long q = base + 32ll * k;
+    acc += ldm(val + q) * xf(ldcol(ix, q, r));
+  }
+  return acc;
+}
+
+// Block partial -> per-block slot; the last block to finish sums the slots in
+// block order and returns true (with the totals in tot[] for every thread).
+template <int ND>
+__device__ __forceinline__ bool grid_reduce(double (&v)[ND], double* __restrict__ part, unsigned* counter,
+                                            double (&tot)[ND]) {
+  __shared__ double red[ND][BI_WARPS];
+  __shared__ int amlast;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int d = 0; d < ND; ++d) {
+    double x = v[d];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if (lane == 0) red[d][wid] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+      double s = 0.0;
+#pragma unroll
+      for (int w = 0; w < BI_WARPS; ++w) s += red[d][w];
+      part[d * gridDim.x + blockIdx.x] = s;
+    }
+    __threadfence();
+    const unsigned t = atomicAdd(counter, 1u);
+    amlast = (t == gridDim.x - 1) ? 1 : 0;
+  }
+  __syncthreads();
+  if (!amlast) return false;
+  __threadfence();
+#pragma unroll
+  for (int d = 0; d < ND; ++d) {
+    double s = 0.0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += BI_BLOCK) s += __ldcg(part + d * gridDim.x + i);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    __syncthreads();
+    if (lane == 0) red[d][wid] = s;
+    __syncthreads();
+    double t = 0.0;
+#pragma unroll
+    for (int w = 0; w < BI_WARPS; ++w) t += red[d][w];
+    tot[d] = t;
+  }
+  if (threadIdx.x == 0) *counter = 0u;
+  return true;
+}
+
+template <typename MT, typename IT, typename VT>
+struct BiArgs {
+  int n;
+  const long long* off;
+  const IT* ix;         // shared by A and M (same pattern)
+  const double* aval;
+  const MT* mval;
+  const double* b;
+  double* x;
+  double* r;
+  VT* rs;
+  VT* p0;
+  VT* p1;
+  VT* y;
+  double* ay;
+  double* s;
+  VT* z;
+  double* az;
+  double* part;
+  Scal* S;
+};
+
+__device__ __forceinline__ bool finished(const Scal* S) { return *(volatile const int*)&S->done != 0; }
+
+__device__ __forceinline__ bool bad(double v) { return !isfinite(v); }
+
+// K0: r = b - A x, r* = r, p = ay = 0, rho = (r*, r), ||r||, ||b||
+template <typename MT, typename IT, typename VT>
+__global__ void __launch_bounds__(BI_BLOCK) k_bi_init(BiArgs<MT, IT, VT> a, double tol, int tol_mode, int maxiter,
+                                                      int verify) {
+  double v[3] = {0.0, 0.0, 0.0};
+  const int stride = gridDim.x * BI_BLOCK;
+  for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) {
+    const double ax = sell_row(a.off, a.aval, a.ix, r, [&](int c) { return ldv(a.x + c); });
+    const double br = a.b[r];
+    const double rr = br + (-1.0) * ax;
+    a.r[r] = rr;
+    const VT rsv = (VT)rr;
+    a.rs[r] = rsv;
+    a.p0[r] = (VT)0.0;
+    a.p1[r] = (VT)0.0;
+    a.ay[r] = 0.0;
+    v[0] += (double)rsv * rr;
+    v[1] += rr * rr;
+    v[2] += br * br;
+  }
+  double tot[3];
+  if (grid_reduce<3>(v, a.part, &a.S->counter[0], tot) && threadIdx.x == 0) {
+    Scal* S = a.S;
+    S->rho = tot[0];
+    S->res = sqrt(tot[1]);
+    S->bnorm = sqrt(tot[2]);
+    S->thr = (tol_mode == DCU_TOL_REL) ? tol * S->bnorm : tol;
+    S->alpha = 0.0;
+    S->omega = 1.0;
+    S->beta = 0.0;
+    S->pidx = 0;
+    S->it = 1;
+    S->maxiter = maxiter;
+    S->verify = verify;
+    S->verify_pending = 0;
+    S->replacements = 0;
+    S->true_res = -1.0;
+    S->status = ST_RUN;
+    S->done = 0;
+    if (S->res == 0.0) {  // x0 already solves the system
+      S->status = DCU_SOLVE_CONVERGED;
+      S->done = 1;
+    } else if (maxiter <= 1) {
+      S->status = DCU_SOLVE_MAXITER;
+      S->done = 1;
+    }
+  }
+}
+
+// K1: p = r + beta (p - omega ay); y = M p
+template <typename MT, typename IT, typename VT>
+__global__ void __launch_bounds__(BI_BLOCK) k_bi_py(BiArgs<MT, IT, VT> a) {
+  if (finished(a.S)) return;
+  const double beta = a.S->beta, omega = a.S->omega;
+  const int pidx = a.S->pidx;
+  const VT* __restrict__ pold = pidx ? a.p1 : a.p0;
+  VT* __restrict__ pnew = pidx ? a.p0 : a.p1;
+  const double* __restrict__ rr = a.r;
+  const double* __restrict__ ay = a.ay;
+  auto pf = [&](int c) { return ldv(rr + c) + beta * (ldv(pold + c) - omega * ldv(ay + c)); };
+  const int stride = gridDim.x * BI_BLOCK;
+  for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) {
+    const double yv = sell_row(a.off, a.mval, a.ix, r, pf);
+    pnew[r] = (VT)pf(r);
+    a.y[r] = (VT)yv;
+  }
+}
+
+// K2: ay = A y; alpha = rho / (r*, ay)
+template <typename MT, typename IT, typename VT>
+__global__ void __launch_bounds__(BI_BLOCK) k_bi_ay(BiArgs<MT, IT, VT> a) {
+  if (finished(a.S)) return;
+  double v[1] = {0.0};
+  const VT* __restrict__ y = a.y;
+  const int stride = gridDim.x * BI_BLOCK;
+  for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) {
+    const double ayv = sell_row(a.off, a.aval, a.ix, r, [&](int c) { return ldv(y + c); });
+    a.ay[r] = ayv;
+    v[0] += (double)a.rs[r] * ayv;
+  }
+  double tot[1];
+  if (grid_reduce<1>(v, a.part, &a.S->counter[1], tot) && threadIdx.x == 0) {
+    Scal* S = a.S;
+    const double alpha = S->rho / tot[0];
+    S->alpha = alpha;
+    if (tot[0] == 0.0 || bad(alpha)) {
+      S->status = DCU_SOLVE_BREAKDOWN;
+      S->done = 1;
+    }
+  }
+}
+
+// K3: s = r - alpha ay; z = M s
+template <typename MT, typename IT, typename VT>
+__global__ void __launch_bounds__(BI_BLOCK) k_bi_sz(BiArgs<MT, IT, VT> a) {
+  if (finished(a.S)) return;
+  const double nalpha = -1.0 * a.S->alpha;
+  const double* __restrict__ rr = a.r;
+  const double* __restrict__ ay = a.ay;
+  auto sf = [&](int c) { return ldv(rr + c) + nalpha * ldv(ay + c); };
+  const int stride = gridDim.x * BI_BLOCK;
+  for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) {
+    const double zv = sell_row(a.off, a.mval, a.ix, r, sf);
+    a.s[r] = rr[r] + nalpha * ay[r];
+    a.z[r] = (VT)zv;
+  }
+}
+
+// K4: az = A z; omega = (az, s) / (az, az)
+template <typename MT, typename IT, typename VT>
+__global__ void __launch_bounds__(BI_BLOCK) k_bi_az(BiArgs<MT, IT, VT> a) {
+  if (finished(a.S)) return;
+  double v[2] = {0.0, 0.0};
+  const VT* __restrict__ z = a.z;
+  const int stride = gridDim.x * BI_BLOCK;
+  for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) {
+    const double azv = sell_row(a.off, a.aval, a.ix, r, [&](int c) { return ldv(z + c); });
+    a.az[r] = azv;
+    v[0] += azv * a.s[r];
+    v[1] += azv * azv;
+  }
+  double tot[2];
+  if (grid_reduce<2>(v, a.part, &a.S->counter[2], tot) && threadIdx.x == 0) {
+    Scal* S = a.S;
+    const double omega = tot[0] / tot[1];
+    S->omega = omega;
+    if (tot[1] == 0.0 || omega == 0.0 || bad(omega)) {
+      S->status = DCU_SOLVE_BREAKDOWN;
+      S->done = 1;
+    }
+  }
+}
+
+// K5: x += alpha y + omega z; r = s - omega az; rho, beta, ||r||, stop test
+template <typename MT, typename IT, typename VT>
+__global__ void __launch_bounds__(BI_BLOCK) k_bi_xr(BiArgs<MT, IT, VT> a) {
+  if (finished(a.S)) return;
+  const double alpha = a.S->alpha, omega = a.S->omega, nomega = -1.0 * omega;
+  double v[2] = {0.0, 0.0};
+  const int stride = gridDim.x * BI_BLOCK;
+  for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) {
+    double xv = a.x[r];
+    xv = xv + alpha * (double)a.y[r];
+    xv = xv + omega * (double)a.z[r];
+    a.x[r] = xv;
+    const double rn = a.s[r] + nomega * a.az[r];
+    a.r[r] = rn;
+    v[0] += (double)a.rs[r] * rn;
+    v[1] += rn * rn;
+  }
+  double tot[2];
+  if (grid_reduce<2>(v, a.part, &a.S->counter[3], tot) && threadIdx.x == 0) {
+    Scal* S = a.S;
+    const double rho_new = tot[0];
+    const double beta = (rho_new / S->rho) * (alpha / omega);
+    S->beta = beta;
+    S->rho = rho_new;
+    S->res = sqrt(tot[1]);
+    S->pidx ^= 1;
+    if (bad(S->res) || bad(beta) || rho_new == 0.0) {
+      S->status = DCU_SOLVE_BREAKDOWN;
+      S->done = 1;
+    } else if (S->res < S->thr) {
+      if (S->verify) S->verify_pending = 1;
+      else S->status = DCU_SOLVE_CONVERGED;
+      S->done = 1;
+    } else {
+      S->it += 1;
+      if (S->it >= S->maxiter) {
+        S->status = DCU_SOLVE_MAXITER;
+        S->done = 1;
+      }
+    }
+  }
+}
+
+// K6: true residual b - A x.  replace = 1: residual replacement after the
+// recurrence met the threshold (continue unless the true residual meets it
+// too); replace = 0: report only.
+template <typename MT, typename IT, typename VT>
+__global__ void __launch_bounds__(BI_BLOCK) k_bi_true(BiArgs<MT, IT, VT> a, int replace) {
+  double v[2] = {0.0, 0.0};
+  const int stride = gridDim.x * BI_BLOCK;
+  for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) {
+    const double ax = sell_row(a.off, a.aval, a.ix, r, [&](int c) { return ldv(a.x + c); });
+    const double rt = a.b[r] - ax;
+    if (replace) a.r[r] = rt;
+    v[0] += (double)a.rs[r] * rt;
+    v[1] += rt * rt;
+  }
+  double tot[2];
+  if (grid_reduce<2>(v, a.part, &a.S->counter[4], tot) && threadIdx.x == 0) {
+    Scal* S = a.S;
+    S->true_res = sqrt(tot[1]);
+    if (replace) {
+      S->verify_pending = 0;
+      if (S->true_res < S->thr) {
+        S->status = DCU_SOLVE_CONVERGED;
+        S->done = 1;
+      } else {
+        S->rho = tot[0];
+        S->res = S->true_res;
+        S->replacements += 1;
+        S->it += 1;
+        if (S->it >= S->maxiter) {
+          S->status = DCU_SOLVE_MAXITER;
+          S->done = 1;
+        } else {
+          S->done = 0;
+        }
+      }
+    }
+  }
+}
+
+template <typename MT, typename IT, typename VT>
+int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval, const IT* ix, const double* b,
+               double* x, const dcu_options* opt, dcu_solve_info* info) {
+  const int n = plan.n;
+  const int grid = waves_grid(c, n, BI_BLOCK, 2048 / BI_BLOCK);
+  // vectors: r, ay, s, az (double) + rs, p0, p1, y, z (VT), 256-byte aligned
+  auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  const size_t nd = al(sizeof(double) * (size_t)n), nv = al(sizeof(VT) * (size_t)n);
+  DCU_TRY(ensure(c, B_VEC, 4 * nd + 5 * nv));
+  DCU_TRY(ensure(c, B_PART, sizeof(double) * 3 * (size_t)grid + 256));
+  DCU_TRY(ensure(c, B_SCAL, sizeof(Scal)));
+  char* base = bp<char>(c, B_VEC);
+  BiArgs<MT, IT, VT> a;
+  a.n = n;
+  a.off = plan.off;
+  a.ix = ix;
+  a.aval = aval;
+  a.mval = mval;
+  a.b = b;
+  a.x = x;
+  a.r = (double*)(base);
+  a.ay = (double*)(base + nd);
+  a.s = (double*)(base + 2 * nd);
+  a.az = (double*)(base + 3 * nd);
+  a.rs = (VT*)(base + 4 * nd);
+  a.p0 = (VT*)(base + 4 * nd + nv);
+  a.p1 = (VT*)(base + 4 * nd + 2 * nv);
+  a.y = (VT*)(base + 4 * nd + 3 * nv);
+  a.z = (VT*)(base + 4 * nd + 4 * nv);
+  a.part = bp<double>(c, B_PART);
+  a.S = bp<Scal>(c, B_SCAL);
+  DCU_CUDA(c, cudaMemsetAsync(a.S, 0, sizeof(Scal), c->stream));
+  int maxiter = opt->maxiter > 0 ? opt->maxiter : n;  // bicgstab_solver.h:134
+  DCU_CUDA(c, cudaEventRecord(c->ev[0], c->stream));
+  k_bi_init<MT, IT, VT><<<grid, BI_BLOCK, 0, c->stream>>>(a, opt->tol, opt->tol_mode, maxiter, opt->verify);
+  DCU_LAUNCHED(c, "k_bi_init");
+
+  // graph of CHUNK_ITERS iterations
+  std::vector<const void*> key = {plan.off, ix, aval, mval, b, x, base, a.part, a.S, (const void*)(intptr_t)n,
+                                  (const void*)(intptr_t)grid};
+  GraphSlot* ge = nullptr;
+  for (auto& e : c->graphs)
+    if (e.key == key) ge = &e;
+  if (!ge) {
+    cudaGraph_t g = nullptr;
+    DCU_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    for (int i = 0; i < CHUNK_ITERS; ++i) {
+      k_bi_py<MT, IT, VT><<<grid, BI_BLOCK, 0, c->stream>>>(a);
+      k_bi_ay<MT, IT, VT><<<grid, BI_BLOCK, 0, c->stream>>>(a);
+      k_bi_sz<MT, IT, VT><<<grid, BI_BLOCK, 0, c->stream>>>(a);
+      k_bi_az<MT, IT, VT><<<grid, BI_BLOCK, 0, c->stream>>>(a);
+      k_bi_xr<MT, IT, VT><<<grid, BI_BLOCK, 0, c->stream>>>(a);
+    }
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture", __FILE__, __LINE__);
+    GraphSlot ne;
+    ne.key = key;
+    ne.nodes = 5 * CHUNK_ITERS;
+    e = cudaGraphInstantiate(&ne.exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaGraphInstantiate", __FILE__, __LINE__);
+    if (c->graphs.size() >= 8) {  // bounded cache: drop the oldest
+      cudaGraphExecDestroy(c->graphs.front().exec);
+      c->graphs.erase(c->graphs.begin());
+    }
+    c->graphs.push_back(ne);
+    ge = &c->graphs.back();
+  }
+
+  // Chunks are launched one ahead of the flag that is read back, so the GPU
+  // never idles on the host; after convergence at most one chunk of
+  // early-exit kernels runs.
+  Scal hs;
+  Scal* pin = reinterpret_cast<Scal*>(c->pinned);
+  int* flag = reinterpret_cast<int*>(reinterpret_cast<char*>(c->pinned) + 1024);
+  // Every chunk either finishes or advances the counter by CHUNK_ITERS, and
+  // each replacement advances it by one, so these bounds are never reached
+  // by a working solver; they turn a logic error into a failure, not a hang.
+  const long long max_chunks = (long long)maxiter / CHUNK_ITERS + 4;
+  for (int restarts = 0;; ++restarts) {
+    if (restarts > maxiter + 1) return fail(c, DCU_ERR_CUDA, "solver did not terminate (restarts)");
+    for (long long i = 0;; ++i) {
+      if (i > max_chunks) return fail(c, DCU_ERR_CUDA, "solver did not terminate (chunks)");
+      DCU_CUDA(c, cudaGraphLaunch(ge->exec, c->stream));
+      c->launches += ge->nodes;
+      DCU_CUDA(c, cudaMemcpyAsync(flag + (i & 1), &a.S->done, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+      DCU_CUDA(c, cudaEventRecord(c->ev[2 + (i & 1)], c->stream));
+      if (i > 0) {
+        DCU_CUDA(c, cudaEventSynchronize(c->ev[2 + ((i - 1) & 1)]));
+        if (flag[(i - 1) & 1]) break;
+      }
+    }
+    DCU_CUDA(c, cudaMemcpyAsync(pin, a.S, sizeof(Scal), cudaMemcpyDeviceToHost, c->stream));
+    DCU_CUDA(c, cudaStreamSynchronize(c->stream));
+    hs = *pin;
+    if (hs.verify_pending) {
+      k_bi_true<MT, IT, VT><<<grid, BI_BLOCK, 0, c->stream>>>(a, 1);
+      DCU_LAUNCHED(c, "k_bi_true");
+      DCU_CUDA(c, cudaMemcpyAsync(pin, a.S, sizeof(Scal), cudaMemcpyDeviceToHost, c->stream));
+      DCU_CUDA(c, cudaStreamSynchronize(c->stream));
+      hs = *pin;
+      if (!hs.done) continue;
+    }
+    break;
+  }
+  if (hs.true_res < 0.0) {
+    k_bi_true<MT, IT, VT><<<grid, BI_BLOCK, 0, c->stream>>>(a, 0);
+    DCU_LAUNCHED(c, "k_bi_true");
+  }
+  DCU_CUDA(c, cudaEventRecord(c->ev[1], c->stream));
+  DCU_CUDA(c, cudaMemcpyAsync(pin, a.S, sizeof(Scal), cudaMemcpyDeviceToHost, c->stream));
+  DCU_CUDA(c, cudaStreamSynchronize(c->stream));
+  hs = *pin;
+  if (info) {
+    info->iters = hs.it;
+    info->status = hs.status;
+    info->replacements = hs.replacements;
+    info->res = hs.res;
+    info->true_res = hs.true_res;
+    info->bnorm = hs.bnorm;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+    info->ms = ms;
+  }
+  return DCU_OK;
+}
+
+}  // namespace
+
+int bicgstab_solve(Ctx* c, const SellPlan& plan, const double* aval_sell, const void* mval_sell, const double* b,
+                   double* x, const dcu_options* opt, dcu_solve_info* info) {
+  if (opt->precision == DCU_PREC_FP64)
+    return run_solver<double, int, double>(c, plan, aval_sell, (const double*)mval_sell, plan.idx, b, x, opt, info);
+  if (opt->precision == DCU_PREC_MIXED_FP32) {
+    if (plan.delta16)
+      return run_solver<float, int16_t, float>(c, plan, aval_sell, (const float*)mval_sell, plan.del, b, x, opt, info);
+    return run_solver<float, int, float>(c, plan, aval_sell, (const float*)mval_sell, plan.idx, b, x, opt, info);
+  }
+  if (plan.delta16)
+    return run_solver<__nv_bfloat16, int16_t, float>(c, plan, aval_sell, (const __nv_bfloat16*)mval_sell, plan.del, b,
+                                                     x, opt, info);
+  return run_solver<__nv_bfloat16, int, float>(c, plan, aval_sell, (const __nv_bfloat16*)mval_sell, plan.idx, b, x,
+                                               opt, info);
+}
+
+void release_graphs(Ctx* c) {
+  for (auto& g : c->graphs) cudaGraphExecDestroy(g.exec);
+  c->graphs.clear();
+}
+
+}  // namespace dcu

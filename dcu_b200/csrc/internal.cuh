@@ -1,0 +1,164 @@
+// Internal declarations of libdcu_spai (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "dcu_spai.h"
+
+namespace dcu {
+
+// ---------------------------------------------------------------------------
+// Device buffer owned by the context; grows on demand, never shrinks.
+// ---------------------------------------------------------------------------
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+enum BufId {
+  B_STATS = 0,     // int stats of the SPAI build
+  B_BIGLIST,       // columns for the CTA kernel
+  B_CHUNKS,        // dynamic-schedule chunk bounds
+  B_SLAB_A,        // CTA kernel dense least-squares slabs
+  B_SLAB_BITS,     // CTA kernel bitmap / prefix slabs
+  B_MVAL,          // internal FP64 M when the caller passes none
+  B_ROWCNT,        // CSR row counts / fill cursors
+  B_RPTR,          // CSR row pointers
+  B_RCOL,          // CSR column indices
+  B_RPERM,         // CSR -> CSC position
+  B_LONGROWS,      // rows too long for the thread sort
+  B_SCAN,          // scan block sums
+  B_SELL_OFF,      // SELL slice offsets (int64)
+  B_SELL_W,        // SELL slice widths
+  B_SELL_IDX,      // SELL absolute column indices
+  B_SELL_DEL,      // SELL 16-bit column deltas
+  B_SELL_PERM,     // SELL slot -> CSC position (-1 padding)
+  B_SELL_AVAL,     // A values in SELL order (FP64)
+  B_SELL_MVAL,     // M values in SELL order (FP64 / FP32 / BF16)
+  B_VEC,           // solver vectors
+  B_PART,          // per-block partial sums
+  B_SCAL,          // solver scalars
+  B_UPLOAD,        // host-API uploads
+  B_SORTTMP,       // global scratch of the long-row sort
+  B_COUNT
+};
+
+// An instantiated CUDA graph and the buffers/sizes it was captured with.
+struct GraphSlot {
+  std::vector<const void*> key;
+  cudaGraphExec_t exec = nullptr;
+  int nodes = 0;
+};
+
+struct Ctx {
+  int device = 0;
+  int sms = 0;
+  int units = 0;
+  int max_threads_sm = 2048;
+  size_t smem_optin = 0;
+  cudaStream_t stream = nullptr;       // the context's own non-blocking stream
+  cudaStream_t user_stream = nullptr;  // caller's stream to order against (optional)
+  cudaEvent_t ev_sync = nullptr;       // ordering between user_stream and stream
+  std::string err;
+  long long launches = 0;
+  DevBuf buf[B_COUNT];
+  void* pinned = nullptr;   // small pinned host scratch (flags, stats), kPinnedBytes
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  std::vector<GraphSlot> graphs;  // BiCGSTAB iteration graphs (bounded cache)
+};
+
+constexpr size_t kPinnedBytes = 4096;
+
+// Error helpers: record the message in the context and return a status.
+int fail(Ctx* c, int code, const char* fmt, ...);
+int cuda_fail(Ctx* c, cudaError_t e, const char* what, const char* file, int line);
+
+#define DCU_CUDA(ctx, call)                                                   \
+  do {                                                                        \
+    cudaError_t e_ = (call);                                                  \
+    if (e_ != cudaSuccess) return ::dcu::cuda_fail(ctx, e_, #call, __FILE__, __LINE__); \
+  } while (0)
+
+#define DCU_LAUNCHED(ctx, name)                                               \
+  do {                                                                        \
+    (ctx)->launches++;                                                        \
+    cudaError_t e_ = cudaGetLastError();                                      \
+    if (e_ != cudaSuccess) return ::dcu::cuda_fail(ctx, e_, name, __FILE__, __LINE__); \
+  } while (0)
+
+#define DCU_TRY(expr)                                                         \
+  do {                                                                        \
+    int s_ = (expr);                                                          \
+    if (s_ != DCU_OK) return s_;                                              \
+  } while (0)
+
+// Ensure buffer `id` holds at least `bytes`; contents are not preserved.
+int ensure(Ctx* c, BufId id, size_t bytes);
+template <typename T>
+inline T* bp(Ctx* c, BufId id) { return reinterpret_cast<T*>(c->buf[id].p); }
+
+// Exclusive scan of int32 counts into int32 (or int64) offsets; out[n] = total.
+int scan_exclusive_i32(Ctx* c, const int* in, int* out, int n);
+int scan_exclusive_i64(Ctx* c, const int* in, long long* out, int n);
+
+// ---------------------------------------------------------------------------
+// Sparse pattern analysis of A (CSC): CSR transpose and SELL-32 layout.
+// ---------------------------------------------------------------------------
+struct SellPlan {
+  int n = 0, nnz = 0;
+  int nslices = 0;
+  long long slots = 0;
+  bool delta16 = false;   // every |col - row| < 32768
+  const long long* off = nullptr;
+  const int* width = nullptr;
+  const int* idx = nullptr;
+  const int16_t* del = nullptr;
+  const int* perm = nullptr;
+};
+
+// Fails with DCU_ERR_ARG unless ptr[0] = 0, ptr is non-decreasing,
+// ptr[n] = nnz and every row index lies in [0, n).  Every entry point runs it
+// before the first kernel that follows the indices.
+int validate_csc(Ctx* c, int n, int nnz, const int* ptr, const int* idx);
+int csr_from_csc(Ctx* c, int n, int nnz, const int* ptr, const int* idx, int* rptr, int* rcol,
+                 int* rperm);
+int csr_values(Ctx* c, int nnz, const int* rperm, const double* val, double* rval);
+int sell_plan(Ctx* c, int n, int nnz, const int* ptr, const int* idx, SellPlan* plan);
+// dst[slot] = (perm[slot] >= 0) ? src[perm[slot]] : 0, converted to the element type.
+int sell_gather_f64(Ctx* c, const SellPlan& p, const double* src, double* dst);
+int sell_gather_f32(Ctx* c, const SellPlan& p, const double* src, float* dst);
+int sell_gather_bf16(Ctx* c, const SellPlan& p, const double* src, __nv_bfloat16* dst);
+
+// ---------------------------------------------------------------------------
+// SPAI build and pattern.
+// ---------------------------------------------------------------------------
+int spai_build(Ctx* c, int n, int nnz, const int* ptr, const int* idx, const double* val,
+               const dcu_options* opt, double* mval, double* colres, dcu_build_info* info);
+int spai_pattern(Ctx* c, int n, const int* ptr, const int* idx, int col_start, int col_end,
+                 int* icount, long long* iptr, int* ilist, long long cap, long long* total);
+
+// ---------------------------------------------------------------------------
+// BiCGSTAB on the SELL plan.
+// ---------------------------------------------------------------------------
+int bicgstab_solve(Ctx* c, const SellPlan& plan, const double* aval_sell, const void* mval_sell,
+                   const double* b, double* x, const dcu_options* opt, dcu_solve_info* info);
+void release_graphs(Ctx* c);
+
+// grid size for grid-stride kernels: whole waves of `per_sm` blocks
+inline int waves_grid(const Ctx* c, long long work_items, int block, int per_sm) {
+  long long need = (work_items + block - 1) / block;
+  long long cap = (long long)c->sms * per_sm;
+  if (need < 1) need = 1;
+  return (int)(need < cap ? need : cap);
+}
+
+}  // namespace dcu
+
+struct dcu_spai_ctx : public dcu::Ctx {};

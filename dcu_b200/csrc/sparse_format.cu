@@ -1,0 +1,354 @@
+// Pattern conversions on the device: CSC -> CSR (the reference's cuCSC2CSR,
+// include/common/cuFormatConversion.h:453-589: per-row counts, a scan, a
+// scatter into row slots, then ascending column order inside each row) and
+// the SELL-32 layout the SpMV kernels read.
+//
+// Layout in HBM (n rows, nnz entries):
+//   CSR    rptr int32[n+1], rcol int32[nnz], rperm int32[nnz] (CSR slot -> CSC slot)
+//   SELL   slice s = rows [32 s, 32 s + 32); width[s] = longest row in the slice;
+//          slot of (row r, k-th entry) = off[s] + 32 k + (r mod 32), so one warp
+//          reads 32 consecutive slots per k (128-byte lines for FP32/int32,
+//          256 bytes for FP64).  Padding slots carry column = r and perm = -1.
+//          del int16 holds col - r when every |col - r| < 32768.
+#include "internal.cuh"
+
+namespace dcu {
+namespace {
+
+__global__ void k_row_count(const int* __restrict__ idx, int nnz, int* __restrict__ cnt) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += gridDim.x * blockDim.x)
+    atomicAdd(&cnt[idx[e]], 1);
+}
+
+// One thread per column: scatter the column's entries into their rows' slots.
+__global__ void k_row_scatter(const int* __restrict__ ptr, const int* __restrict__ idx, int n,
+                              const int* __restrict__ rptr, int* __restrict__ fill,
+                              int* __restrict__ rcol, int* __restrict__ rperm) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+    for (int e = ptr[c]; e < ptr[c + 1]; ++e) {
+      int r = idx[e];
+      int pos = rptr[r] + atomicAdd(&fill[r], 1);
+      rcol[pos] = c;
+      rperm[pos] = e;
+    }
+  }
+}
+
+constexpr int kThreadSortMax = 64;
+
+// Rows up to kThreadSortMax entries: insertion sort by one thread; longer rows
+// are queued for the block sort.  Column indices inside a row are distinct
+// (a CSC column lists each row once), so the order is unique.
+__global__ void k_row_sort_short(const int* __restrict__ rptr, int n, int* __restrict__ rcol,
+                                 int* __restrict__ rperm, int* __restrict__ long_rows,
+                                 int* __restrict__ long_count) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    int s = rptr[r], e = rptr[r + 1];
+    int len = e - s;
+    if (len > kThreadSortMax) {
+      long_rows[atomicAdd(long_count, 1)] = r;
+      atomicMax(long_count + 1, len);
+      continue;
+    }
+    for (int i = s + 1; i < e; ++i) {
+      int kc = rcol[i], kp = rperm[i];
+      int j = i - 1;
+      while (j >= s && rcol[j] > kc) {
+        rcol[j + 1] = rcol[j];
+        rperm[j + 1] = rperm[j];
+        --j;
+      }
+      rcol[j + 1] = kc;
+      rperm[j + 1] = kp;
+    }
+  }
+}
+
+// One block per long row: bitonic sort of (col << 32 | perm) keys in shared
+// memory (rows up to kSmemSortMax) or in a global scratch slab.
+constexpr int kSmemSortMax = 8192;
+
+__device__ __forceinline__ void bitonic_block(unsigned long long* key, int npow2) {
+  for (int k = 2; k <= npow2; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = threadIdx.x; i < npow2; i += blockDim.x) {
+        int l = i ^ j;
+        if (l > i) {
+          unsigned long long a = key[i], b = key[l];
+          bool up = (i & k) == 0;
+          if ((a > b) == up) {
+            key[i] = b;
+            key[l] = a;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+__global__ void __launch_bounds__(512) k_row_sort_long(const int* __restrict__ rptr, const int* __restrict__ rows,
+                                                       const int* __restrict__ count, int* __restrict__ rcol,
+                                                       int* __restrict__ rperm, unsigned long long* __restrict__ gscratch,
+                                                       long long gscratch_per_block) {
+  extern __shared__ unsigned long long skey[];
+  int nrows = *count;
+  for (int q = blockIdx.x; q < nrows; q += gridDim.x) {
+    int r = rows[q];
+    int s = rptr[r], len = rptr[r + 1] - s;
+    int np2 = 1;
+    while (np2 < len) np2 <<= 1;
+    unsigned long long* key = (np2 <= kSmemSortMax) ? skey : gscratch + (long long)blockIdx.x * gscratch_per_block;
+    for (int i = threadIdx.x; i < np2; i += blockDim.x)
+      key[i] = (i < len) ? ((unsigned long long)(unsigned)rcol[s + i] << 32 | (unsigned)rperm[s + i]) : ~0ull;
+    __syncthreads();
+    bitonic_block(key, np2);
+    for (int i = threadIdx.x; i < len; i += blockDim.x) {
+      rcol[s + i] = (int)(key[i] >> 32);
+      rperm[s + i] = (int)(key[i] & 0xffffffffu);
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void k_gather_f64(const int* __restrict__ perm, const double* __restrict__ src, int nnz,
+                             double* __restrict__ dst) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += gridDim.x * blockDim.x) dst[e] = src[perm[e]];
+}
+
+// SELL: slice widths (max row length of each 32-row slice), one warp per slice.
+__global__ void k_sell_width(const int* __restrict__ rptr, int n, int nslices, int* __restrict__ width) {
+  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int s = warp; s < nslices; s += nw) {
+    int r = s * 32 + lane;
+    int len = (r < n) ? rptr[r + 1] - rptr[r] : 0;
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) len = max(len, __shfl_xor_sync(0xffffffffu, len, d));
+    if (lane == 0) width[s] = len * 32;  // slots in the slice (scanned into offsets)
+  }
+}
+
+__global__ void k_sell_fill(const int* __restrict__ rptr, const int* __restrict__ rcol, const int* __restrict__ rperm,
+                            int n, int nslices, const long long* __restrict__ off, int* __restrict__ sidx,
+                            int* __restrict__ sperm, int* __restrict__ maxdelta) {
+  int rows_total = nslices * 32;
+  int local_max = 0;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows_total; r += gridDim.x * blockDim.x) {
+    int s = r >> 5, lane = r & 31;
+    long long base = off[s] + lane;
+    int w = (int)((off[s + 1] - off[s]) >> 5);
+    int rs = 0, len = 0;
+    if (r < n) {
+      rs = rptr[r];
+      len = rptr[r + 1] - rs;
+    }
+    int self = (r < n) ? r : 0;
+    for (int k = 0; k < w; ++k) {
+      long long q = base + 32ll * k;
+      if (k < len) {
+        int col = rcol[rs + k];
+        sidx[q] = col;
+        sperm[q] = rperm[rs + k];
+        int d = abs(col - self);
+        local_max = max(local_max, d);
+      } else {
+        sidx[q] = self;
+        sperm[q] = -1;
+      }
+    }
+  }
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) local_max = max(local_max, __shfl_xor_sync(0xffffffffu, local_max, d));
+  if ((threadIdx.x & 31) == 0) atomicMax(maxdelta, local_max);
+}
+
+__global__ void k_sell_delta(const int* __restrict__ sidx, long long slots, int n, int nslices,
+                             const long long* __restrict__ off, int16_t* __restrict__ del) {
+  // slot q belongs to row 32 s + ((q - off[s]) mod 32); recover s by walking
+  // per row instead: one thread per (row, k) over whole slices.
+  int rows_total = nslices * 32;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows_total; r += gridDim.x * blockDim.x) {
+    int s = r >> 5, lane = r & 31;
+    long long base = off[s] + lane;
+    int w = (int)((off[s + 1] - off[s]) >> 5);
+    int self = (r < n) ? r : 0;
+    for (int k = 0; k < w; ++k) {
+      long long q = base + 32ll * k;
+      del[q] = (int16_t)(sidx[q] - self);
+    }
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ T cvt_from_double(double v);
+template <>
+__device__ __forceinline__ double cvt_from_double<double>(double v) { return v; }
+template <>
+__device__ __forceinline__ float cvt_from_double<float>(double v) { return (float)v; }
+template <>
+__device__ __forceinline__ __nv_bfloat16 cvt_from_double<__nv_bfloat16>(double v) { return __double2bfloat16(v); }
+
+template <typename T>
+__global__ void k_sell_gather(const int* __restrict__ sperm, long long slots, const double* __restrict__ src,
+                              T* __restrict__ dst) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < slots;
+       q += (long long)gridDim.x * blockDim.x) {
+    int p = sperm[q];
+    dst[q] = cvt_from_double<T>(p >= 0 ? src[p] : 0.0);
+  }
+}
+
+template <typename T>
+int sell_gather(Ctx* c, const SellPlan& p, const double* src, T* dst) {
+  int grid = waves_grid(c, p.slots, 256, 8);
+  k_sell_gather<T><<<grid, 256, 0, c->stream>>>(p.perm, p.slots, src, dst);
+  DCU_LAUNCHED(c, "k_sell_gather");
+  return DCU_OK;
+}
+
+// Structural check of a CSC matrix before any kernel chases its indices:
+// ptr[0] == 0, ptr non-decreasing, ptr[n] == nnz, 0 <= idx < n.
+__global__ void k_validate_csc(const int* __restrict__ ptr, const int* __restrict__ idx, int n, int nnz,
+                               int* __restrict__ bad) {
+  const int stride = gridDim.x * blockDim.x;
+  int b = 0;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c <= n; c += stride) {
+    const int p = ptr[c];
+    if (c == 0 && p != 0) b |= 1;
+    if (c == n && p != nnz) b |= 2;
+    if (c < n && ptr[c + 1] < p) b |= 4;
+  }
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += stride) {
+    const int r = idx[e];
+    if (r < 0 || r >= n) b |= 8;
+  }
+  if (b) atomicOr(bad, b);
+}
+
+}  // namespace
+
+int validate_csc(Ctx* c, int n, int nnz, const int* ptr, const int* idx) {
+  DCU_TRY(ensure(c, B_ROWCNT, sizeof(int) * (size_t)(n + 1)));
+  int* bad = bp<int>(c, B_ROWCNT);
+  DCU_CUDA(c, cudaMemsetAsync(bad, 0, sizeof(int), c->stream));
+  k_validate_csc<<<waves_grid(c, (long long)(nnz > n ? nnz : n + 1), 256, 8), 256, 0, c->stream>>>(ptr, idx, n, nnz,
+                                                                                                   bad);
+  DCU_LAUNCHED(c, "k_validate_csc");
+  DCU_CUDA(c, cudaMemcpyAsync(c->pinned, bad, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  DCU_CUDA(c, cudaStreamSynchronize(c->stream));
+  const int b = *(int*)c->pinned;
+  if (b) {
+    return fail(c, DCU_ERR_ARG, "malformed CSC matrix:%s%s%s%s", (b & 1) ? " ptr[0] != 0;" : "",
+                (b & 2) ? " ptr[n] != nnz;" : "", (b & 4) ? " ptr decreases;" : "",
+                (b & 8) ? " row index out of [0, n);" : "");
+  }
+  return DCU_OK;
+}
+
+int csr_from_csc(Ctx* c, int n, int nnz, const int* ptr, const int* idx, int* rptr, int* rcol, int* rperm) {
+  DCU_TRY(ensure(c, B_ROWCNT, sizeof(int) * (size_t)(n + 1)));
+  DCU_TRY(ensure(c, B_LONGROWS, sizeof(int) * (size_t)(n + 2)));
+  int* cnt = bp<int>(c, B_ROWCNT);
+  int* longrows = bp<int>(c, B_LONGROWS);
+  int* longcount = longrows + n;  // [0] = count, [1] = longest length
+  DCU_CUDA(c, cudaMemsetAsync(cnt, 0, sizeof(int) * (size_t)(n + 1), c->stream));
+  DCU_CUDA(c, cudaMemsetAsync(longcount, 0, 2 * sizeof(int), c->stream));
+  if (nnz > 0) {
+    k_row_count<<<waves_grid(c, nnz, 256, 8), 256, 0, c->stream>>>(idx, nnz, cnt);
+    DCU_LAUNCHED(c, "k_row_count");
+  }
+  DCU_TRY(scan_exclusive_i32(c, cnt, rptr, n));
+  DCU_CUDA(c, cudaMemsetAsync(cnt, 0, sizeof(int) * (size_t)(n + 1), c->stream));
+  k_row_scatter<<<waves_grid(c, n, 256, 8), 256, 0, c->stream>>>(ptr, idx, n, rptr, cnt, rcol, rperm);
+  DCU_LAUNCHED(c, "k_row_scatter");
+  k_row_sort_short<<<waves_grid(c, n, 256, 8), 256, 0, c->stream>>>(rptr, n, rcol, rperm, longrows, longcount);
+  DCU_LAUNCHED(c, "k_row_sort_short");
+  // Long rows: the block sort needs the longest row for its global slab.
+  DCU_CUDA(c, cudaMemcpyAsync(c->pinned, longcount, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  DCU_CUDA(c, cudaStreamSynchronize(c->stream));
+  int nlong = ((int*)c->pinned)[0];
+  int maxlen = ((int*)c->pinned)[1];
+  if (nlong > 0) {
+    long long np2 = 1;
+    while (np2 < maxlen) np2 <<= 1;
+    int blocks = nlong < c->sms ? nlong : c->sms;
+    long long per_block = (np2 > kSmemSortMax) ? np2 : 0;
+    if (per_block > 0) DCU_TRY(ensure(c, B_SORTTMP, sizeof(unsigned long long) * (size_t)per_block * blocks));
+    unsigned long long* g = per_block > 0 ? bp<unsigned long long>(c, B_SORTTMP) : nullptr;
+    size_t smem = sizeof(unsigned long long) * kSmemSortMax;
+    DCU_CUDA(c, cudaFuncSetAttribute(k_row_sort_long, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_row_sort_long<<<blocks, 512, smem, c->stream>>>(rptr, longrows, longcount, rcol, rperm, g, per_block);
+    DCU_LAUNCHED(c, "k_row_sort_long");
+  }
+  return DCU_OK;
+}
+
+int sell_plan(Ctx* c, int n, int nnz, const int* ptr, const int* idx, SellPlan* plan) {
+  DCU_TRY(ensure(c, B_RPTR, sizeof(int) * (size_t)(n + 1)));
+  DCU_TRY(ensure(c, B_RCOL, sizeof(int) * (size_t)(nnz > 0 ? nnz : 1)));
+  DCU_TRY(ensure(c, B_RPERM, sizeof(int) * (size_t)(nnz > 0 ? nnz : 1)));
+  int* rptr = bp<int>(c, B_RPTR);
+  int* rcol = bp<int>(c, B_RCOL);
+  int* rperm = bp<int>(c, B_RPERM);
+  DCU_TRY(csr_from_csc(c, n, nnz, ptr, idx, rptr, rcol, rperm));
+  int nslices = (n + 31) / 32;
+  DCU_TRY(ensure(c, B_SELL_W, sizeof(int) * (size_t)(nslices + 1)));
+  DCU_TRY(ensure(c, B_SELL_OFF, sizeof(long long) * (size_t)(nslices + 1)));
+  int* width = bp<int>(c, B_SELL_W);
+  long long* off = bp<long long>(c, B_SELL_OFF);
+  k_sell_width<<<waves_grid(c, (long long)nslices * 32, 256, 8), 256, 0, c->stream>>>(rptr, n, nslices, width);
+  DCU_LAUNCHED(c, "k_sell_width");
+  DCU_TRY(scan_exclusive_i64(c, width, off, nslices));
+  DCU_CUDA(c, cudaMemcpyAsync(c->pinned, off + nslices, sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
+  DCU_CUDA(c, cudaStreamSynchronize(c->stream));
+  long long slots = *(long long*)c->pinned;
+  DCU_TRY(ensure(c, B_SELL_IDX, sizeof(int) * (size_t)(slots > 0 ? slots : 1)));
+  DCU_TRY(ensure(c, B_SELL_PERM, sizeof(int) * (size_t)(slots > 0 ? slots : 1)));
+  int* sidx = bp<int>(c, B_SELL_IDX);
+  int* sperm = bp<int>(c, B_SELL_PERM);
+  int* maxdelta = bp<int>(c, B_ROWCNT);  // row counts are no longer needed
+  DCU_CUDA(c, cudaMemsetAsync(maxdelta, 0, sizeof(int), c->stream));
+  k_sell_fill<<<waves_grid(c, (long long)nslices * 32, 256, 8), 256, 0, c->stream>>>(rptr, rcol, rperm, n, nslices, off,
+                                                                                     sidx, sperm, maxdelta);
+  DCU_LAUNCHED(c, "k_sell_fill");
+  DCU_CUDA(c, cudaMemcpyAsync(c->pinned, maxdelta, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  DCU_CUDA(c, cudaStreamSynchronize(c->stream));
+  int md = *(int*)c->pinned;
+  plan->delta16 = md < 32768;
+  plan->del = nullptr;
+  if (plan->delta16) {
+    DCU_TRY(ensure(c, B_SELL_DEL, sizeof(int16_t) * (size_t)(slots > 0 ? slots : 1)));
+    int16_t* del = bp<int16_t>(c, B_SELL_DEL);
+    k_sell_delta<<<waves_grid(c, (long long)nslices * 32, 256, 8), 256, 0, c->stream>>>(sidx, slots, n, nslices, off,
+                                                                                        del);
+    DCU_LAUNCHED(c, "k_sell_delta");
+    plan->del = del;
+  }
+  plan->n = n;
+  plan->nnz = nnz;
+  plan->nslices = nslices;
+  plan->slots = slots;
+  plan->off = off;
+  plan->width = width;
+  plan->idx = sidx;
+  plan->perm = sperm;
+  return DCU_OK;
+}
+
+int sell_gather_f64(Ctx* c, const SellPlan& p, const double* src, double* dst) { return sell_gather<double>(c, p, src, dst); }
+int sell_gather_f32(Ctx* c, const SellPlan& p, const double* src, float* dst) { return sell_gather<float>(c, p, src, dst); }
+int sell_gather_bf16(Ctx* c, const SellPlan& p, const double* src, __nv_bfloat16* dst) {
+  return sell_gather<__nv_bfloat16>(c, p, src, dst);
+}
+
+// CSR with values, for the C ABI (dcu_csc_to_csr_d).
+int csr_values(Ctx* c, int nnz, const int* rperm, const double* val, double* rval) {
+  if (nnz <= 0 || !rval) return DCU_OK;
+  k_gather_f64<<<waves_grid(c, nnz, 256, 8), 256, 0, c->stream>>>(rperm, val, nnz, rval);
+  DCU_LAUNCHED(c, "k_gather_f64");
+  return DCU_OK;
+}
+
+}  // namespace dcu

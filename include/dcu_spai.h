@@ -1,0 +1,208 @@
+/*
+ * dcu_spai.h -- C ABI of the B200 SPAI-preconditioned BiCGSTAB library
+ * (libdcu_spai.so).  Plain pointers and sizes only; every function returns a
+ * dcu_status code and never exits the process.
+ *
+ * Reference interfaces this layer replaces (SingkiWong/DCU):
+ *   dcu_spai_create / dcu_spai_destroy
+ *       initMultiDCU / cleanupMultiDCU        src/spai_multi_dcu.cpp:1296-1350, 2335-2380
+ *   dcu_spai_distribute_columns
+ *       distributeColumns                     src/spai_multi_dcu.cpp:1356-1449
+ *   dcu_spai_build_d / dcu_spai_build_h
+ *       StaticSPAIv20 (single-pass semantics) src/spai_single_dcu.cpp:1224-2687,
+ *       reached through RunStatic/DynamicSPAI_MultiDCU_MPI
+ *                                             src/spai_multi_dcu.cpp:1867-1875
+ *   dcu_spai_pattern_d
+ *       computeJ_SSPAIv10 + computeI*_Symbol_SpMMv1
+ *                                             src/spai_multi_dcu.cpp:275-319, 321-834
+ *   dcu_csc_to_csr_d
+ *       cuCSC2CSR                             include/common/cuFormatConversion.h:453-589
+ *   dcu_bicgstab_d / dcu_bicgstab_h
+ *       cublas2_pbicgstabv2                   include/bicgstab/bicgstab_solver.h:33-275
+ *       (driven as in runBiCGSTABOnRank0      src/spai_multi_dcu.cpp:1878-1951)
+ *   dcu_spai_solve_d / dcu_spai_solve_h
+ *       the whole path: SPAI build, CSC->CSR, BiCGSTAB
+ *
+ * Matrices are square, CSC, 0-based: ptr[n+1] (int32), idx[nnz] row indices
+ * (int32), val[nnz] (float64) -- the CSC_Matrix layout of
+ * include/common/dataType.h:33-41.  The preconditioner M has A's pattern, so
+ * it is passed as values only (mval[nnz], aligned with A's idx).
+ * Suffix _d: device pointers (cudaMalloc'ed, on the context's device);
+ * suffix _h: host pointers (copies are made inside the call).
+ */
+#ifndef DCU_SPAI_H
+#define DCU_SPAI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct dcu_spai_ctx dcu_spai_ctx;
+
+typedef enum {
+  DCU_OK = 0,
+  DCU_ERR_ARG = 1,        /* invalid argument (sizes, pointers, ranges)   */
+  DCU_ERR_CUDA = 2,       /* a CUDA call failed; see dcu_spai_last_error  */
+  DCU_ERR_ALLOC = 3,      /* device or host allocation failed             */
+  DCU_ERR_NO_DEVICE = 4,  /* no CUDA device / device index out of range   */
+  DCU_ERR_LIMIT = 5       /* a size exceeds a documented limit            */
+} dcu_status;
+
+/* Column schedules of the device work queue (the reference's partitions). */
+typedef enum {
+  DCU_SCHED_BALANCED_COLUMNS = 0, /* static: equal contiguous column counts   */
+  DCU_SCHED_BALANCED_NNZ = 1      /* dynamic: nnz-balanced chunks, atomic pull */
+} dcu_schedule;
+
+/* Precision forms. */
+typedef enum {
+  DCU_PREC_FP64 = 0,      /* plain: FP64 least squares, FP64 M, FP64 vectors, int32 indices */
+  DCU_PREC_MIXED_FP32 = 1,/* FP32 least squares, M stored FP32, FP32 preconditioned vectors,
+                             16-bit index deltas where they fit; FP64 A, residual, dots   */
+  DCU_PREC_MIXED_BF16 = 2 /* as MIXED_FP32 with M stored as BF16                           */
+} dcu_precision;
+
+/* Stopping rule. */
+typedef enum {
+  DCU_TOL_ABS = 0,        /* ||r||_2 < tol (the reference, bicgstab_solver.h:229) */
+  DCU_TOL_REL = 1         /* ||r||_2 < tol * ||b||_2                             */
+} dcu_tol_mode;
+
+/* Solver outcome codes (dcu_solve_info.status). */
+typedef enum {
+  DCU_SOLVE_CONVERGED = 0,
+  DCU_SOLVE_MAXITER = 1,
+  DCU_SOLVE_BREAKDOWN = 2 /* rho, (r*,Ay), (Az,Az) or omega zero / non-finite */
+} dcu_solve_status;
+
+typedef struct {
+  int cols_total;         /* columns built                                        */
+  int cols_small;         /* columns solved by the warp-group kernel              */
+  int cols_large;         /* columns solved by the CTA kernel                     */
+  int cols_singular;      /* columns with a zero / non-finite Householder pivot   */
+  int max_nj;             /* max |J_k|                                            */
+  int max_ni;             /* max |I_k|                                            */
+  float ms;               /* device time of the build (CUDA events)              */
+} dcu_build_info;
+
+typedef struct {
+  int iters;              /* the reference's counter (starts at 1; see dcu_bicgstab_d) */
+  int status;             /* dcu_solve_status                                          */
+  int replacements;       /* residual replacements performed                          */
+  double res;             /* recurrence ||r||_2 at exit                                */
+  double true_res;        /* ||b - A x||_2 recomputed in FP64 at exit                  */
+  double bnorm;           /* ||b||_2                                                   */
+  float ms;               /* device time of the solve (CUDA events)                   */
+} dcu_solve_info;
+
+typedef struct {
+  int schedule;           /* dcu_schedule                                   */
+  int precision;          /* dcu_precision                                  */
+  int tol_mode;           /* dcu_tol_mode                                   */
+  int maxiter;            /* <= 0 means n, as the reference (:134)           */
+  double tol;
+  int verify;             /* 1: on recurrence convergence recompute b - A x in
+                             FP64 and continue from it unless it also meets
+                             the threshold (residual replacement); 0: stop on
+                             the recurrence residual exactly as the reference */
+  int col_start, col_end; /* SPAI column range; col_end <= 0 means n          */
+} dcu_options;
+
+/* Fill *opt with the defaults of the BASELINE configs: balanced_columns,
+ * FP64, relative tol 1e-8, maxiter 1000, verify on, all columns. */
+void dcu_options_default(dcu_options* opt);
+
+/* ---- context ------------------------------------------------------------- */
+
+/* Create a context on CUDA device `device`.  `units` is the schedule's unit
+ * count P (the reference's numDCUs); <= 0 picks 4 warp-groups per resident
+ * warp slot of the device.  Replaces initMultiDCU. */
+int dcu_spai_create(dcu_spai_ctx** ctx, int device, int units);
+/* Frees every device buffer the context owns.  Replaces cleanupMultiDCU. */
+void dcu_spai_destroy(dcu_spai_ctx* ctx);
+/* Last error message of this context ("" when none). */
+const char* dcu_spai_last_error(const dcu_spai_ctx* ctx);
+/* Use `stream` (a cudaStream_t) for all work of this context; NULL = the
+ * context's own stream. */
+int dcu_spai_set_stream(dcu_spai_ctx* ctx, void* stream);
+/* Number of work units the schedules split columns over. */
+int dcu_spai_units(const dcu_spai_ctx* ctx);
+/* Number of kernel launches this context has issued (diagnostic counter). */
+long long dcu_spai_launch_count(const dcu_spai_ctx* ctx);
+
+/* Column split of [col_start, col_end) over `units` (host arrays starts/ends
+ * of length units), identical to distributeColumns: schedule 0 =
+ * balanced_columns, 1 = balanced_nnz.  `ptr` is a host array. */
+int dcu_spai_distribute_columns(const int* ptr, int col_start, int col_end, int units,
+                                int schedule, int* starts, int* ends);
+
+/* ---- SPAI ------------------------------------------------------------------ */
+
+/* Pattern pass: |I_k| (icount[k - col_start]) and, when ilist != NULL, the
+ * sorted rows of I_k at ilist[iptr[k - col_start]] where iptr is the
+ * exclusive prefix of icount (written by this call, length ncols + 1,
+ * int64).  Call with ilist == NULL first to learn *total.  Device pointers. */
+int dcu_spai_pattern_d(dcu_spai_ctx* ctx, int n, const int* ptr, const int* idx, int col_start,
+                       int col_end, int* icount, long long* iptr, int* ilist,
+                       long long ilist_capacity, long long* total);
+
+/* SPAI build on A's pattern: mval[nnz] (device, FP64) receives M's values in
+ * A's CSC order; columns outside [opt->col_start, opt->col_end) are zero.
+ * colres (device, optional, length ncols) receives ||A m_k - e_k||_2.
+ * Uses opt->schedule and opt->precision (FP32 least squares for the mixed
+ * forms; mval is FP64 either way). */
+int dcu_spai_build_d(dcu_spai_ctx* ctx, int n, int nnz, const int* ptr, const int* idx,
+                     const double* val, const dcu_options* opt, double* mval, double* colres,
+                     dcu_build_info* info);
+int dcu_spai_build_h(dcu_spai_ctx* ctx, int n, int nnz, const int* ptr, const int* idx,
+                     const double* val, const dcu_options* opt, double* mval, double* colres,
+                     dcu_build_info* info);
+
+/* CSC -> CSR (ascending columns inside each row, values carried along).
+ * Device pointers; rptr[n+1], ridx[nnz], rval[nnz] (rval may be NULL). */
+int dcu_csc_to_csr_d(dcu_spai_ctx* ctx, int n, int nnz, const int* ptr, const int* idx,
+                     const double* val, int* rptr, int* ridx, double* rval);
+
+/* ---- BiCGSTAB --------------------------------------------------------------- */
+
+/* Right-preconditioned BiCGSTAB for A x = b with preconditioner M (values on
+ * A's pattern).  x holds x0 on entry and the solution on exit.  The iteration
+ * counter follows the reference: it starts at 1, the loop runs while
+ * iters < maxiter, and stops when the residual meets the threshold.
+ * opt->precision selects how M and the preconditioned vectors are stored. */
+int dcu_bicgstab_d(dcu_spai_ctx* ctx, int n, int nnz, const int* ptr, const int* idx,
+                   const double* val, const double* mval, const double* b, double* x,
+                   const dcu_options* opt, dcu_solve_info* info);
+int dcu_bicgstab_h(dcu_spai_ctx* ctx, int n, int nnz, const int* ptr, const int* idx,
+                   const double* val, const double* mval, const double* b, double* x,
+                   const dcu_options* opt, dcu_solve_info* info);
+
+/* The whole path: SPAI build of M on A's pattern, then BiCGSTAB.  mval
+ * (optional) receives M (FP64, A's CSC order).  Device pointers. */
+int dcu_spai_solve_d(dcu_spai_ctx* ctx, int n, int nnz, const int* ptr, const int* idx,
+                     const double* val, const double* b, double* x, const dcu_options* opt,
+                     double* mval, dcu_build_info* binfo, dcu_solve_info* sinfo);
+/* Same with host buffers: uploads A and b, runs, downloads x (and mval when
+ * non-NULL). */
+int dcu_spai_solve_h(dcu_spai_ctx* ctx, int n, int nnz, const int* ptr, const int* idx,
+                     const double* val, const double* b, double* x, const dcu_options* opt,
+                     double* mval, dcu_build_info* binfo, dcu_solve_info* sinfo);
+
+/* ---- MatrixMarket input (command-line driver) --------------------------------- */
+
+/* Read a MatrixMarket file into host CSC arrays with the semantics of
+ * readMatrixToCSC (include/common/read.h:1296-1320): "symmetric" in the first
+ * line mirrors off-diagonal entries, explicit zeros are dropped, entries keep
+ * file order inside each column, indices become 0-based.  Arrays are
+ * malloc'ed; release each with dcu_mtx_free.  Returns 0 on success. */
+int dcu_mtx_read(const char* path, int* n, int* nnz, int** ptr, int** idx, double** val);
+void dcu_mtx_free(void* p);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DCU_SPAI_H */

@@ -1,0 +1,89 @@
+"""BiCGSTAB: iteration count within +-1 of the oracle, residual below tol."""
+import numpy as np
+import pytest
+
+import oracle
+from dcu_b200 import native as N
+from dcu_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def test_config1_reference_settings(ctx):
+    # b = 1, x0 = 1, ||r|| < 1e-7 absolute (runBiCGSTABOnRank0)
+    A = W.convdiff2d(64, 10.0)
+    m_o, _, _, _ = oracle.spai(A, "mgs")
+    ref = oracle.bicgstab(A, m_o, np.ones(A.n), np.ones(A.n), tol=1e-7, tol_mode="abs", maxiter=10000)
+    m, _, _ = ctx.build_h(A)
+    x, info = ctx.bicgstab_h(A, m, np.ones(A.n), np.ones(A.n), tol=1e-7, tol_mode=N.TOL_ABS, maxiter=10000, verify=0)
+    assert info.status == N.SOLVE_CONVERGED
+    assert abs(info.iters - ref["iters"]) <= 1
+    assert ref["iters"] == 43
+    assert info.res < 1e-7
+
+
+@pytest.mark.parametrize("prec", [N.PREC_FP64, N.PREC_MIXED_FP32, N.PREC_MIXED_BF16])
+def test_config1_solve(ctx, prec):
+    A = W.convdiff2d(64, 10.0)
+    b = W.rhs_ones_product(A)
+    m_o, _, _, _ = oracle.spai(A, "mgs")
+    ref = oracle.bicgstab(A, m_o, b, None, tol=1e-8, tol_mode="rel", maxiter=1000)
+    x, _, bi, si = ctx.solve_h(A, b, precision=prec)
+    assert si.status == N.SOLVE_CONVERGED
+    relres = np.linalg.norm(b - A.matvec(x)) / np.linalg.norm(b)
+    assert relres < 1e-8
+    assert si.true_res / si.bnorm < 1e-8
+    if prec == N.PREC_FP64:
+        assert abs(si.iters - ref["iters"]) <= 1
+    else:
+        assert abs(si.iters - ref["iters"]) <= max(3, ref["iters"] // 10)
+    assert np.max(np.abs(x - 1.0)) < 1e-5
+
+
+def test_circuit_like(ctx):
+    A = W.circuit_like()
+    rng = np.random.Generator(np.random.PCG64(11))
+    b = rng.uniform(-1, 1, A.n)
+    m_o, _, _, _ = oracle.spai(A, "mgs")
+    ref = oracle.bicgstab(A, m_o, b, None, tol=1e-8, tol_mode="rel", maxiter=1000)
+    x, _, bi, si = ctx.solve_h(A, b)
+    assert si.status == N.SOLVE_CONVERGED
+    assert abs(si.iters - ref["iters"]) <= 1
+    assert np.linalg.norm(b - A.matvec(x)) / np.linalg.norm(b) < 1e-8
+
+
+def test_3d_small(ctx):
+    A = W.convdiff3d(24, 20.0)
+    b, xt = W.rhs_from_solution(A)
+    m_o, _, _, _ = oracle.spai(A, "mgs")
+    ref = oracle.bicgstab(A, m_o, b, None, tol=1e-8, tol_mode="rel", maxiter=1000)
+    for prec in (N.PREC_FP64, N.PREC_MIXED_BF16):
+        x, _, bi, si = ctx.solve_h(A, b, precision=prec)
+        assert si.status == N.SOLVE_CONVERGED
+        assert np.linalg.norm(b - A.matvec(x)) / np.linalg.norm(b) < 1e-8
+        if prec == N.PREC_FP64:
+            assert abs(si.iters - ref["iters"]) <= 1
+
+
+def test_maxiter_counter(ctx):
+    A = W.convdiff2d(64, 10.0)
+    b = W.rhs_ones_product(A)
+    m, _, _ = ctx.build_h(A)
+    x, info = ctx.bicgstab_h(A, m, b, maxiter=5, tol=1e-30, verify=0)
+    assert info.status == N.SOLVE_MAXITER
+    assert info.iters == 5   # the reference's counter runs 1..MAX_ITER
+
+
+def test_csr_matches_oracle(ctx):
+    import torch
+
+    A = W.circuit_like()
+    rp_o, ri_o, rv_o = oracle.csc2csr(A.n, A.ptr, A.idx, A.val)
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    rp = torch.zeros(A.n + 1, dtype=torch.int32, device="cuda")
+    ri = torch.zeros(A.nnz, dtype=torch.int32, device="cuda")
+    rv = torch.zeros(A.nnz, dtype=torch.float64, device="cuda")
+    ctx.csc_to_csr_d(A.n, A.nnz, d(A.ptr), d(A.idx), d(A.val), rp, ri, rv)
+    assert np.array_equal(rp.cpu().numpy(), rp_o)
+    assert np.array_equal(ri.cpu().numpy(), ri_o)
+    assert np.array_equal(rv.cpu().numpy(), rv_o)

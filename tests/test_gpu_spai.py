@@ -1,0 +1,75 @@
+"""SPAI build (gather + Householder QR + solve + scatter) against the oracle."""
+import numpy as np
+import pytest
+
+import oracle
+from dcu_b200 import native as N
+from dcu_b200 import workloads as W
+from tests.test_gpu_pattern import random_csc
+
+pytestmark = pytest.mark.gpu
+
+RTOL_FP64 = 1e-10   # M values, FP64 form, relative to max |M| of the column set
+RTOL_FP32 = 2e-4    # FP32 least squares
+
+
+def rel_err(a, b):
+    return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
+
+
+@pytest.mark.parametrize("name,A", [
+    ("cd2d_64", W.convdiff2d(64, 10.0)),
+    ("cd3d_16", W.convdiff3d(16, 20.0)),
+    ("circuit", W.circuit_like()),
+    ("varcoef_32", W.varcoef2d(32, seed=3)),
+])
+def test_spai_fp64_matches_oracle(ctx, name, A):
+    m_o, res_o, E_o, sing_o = oracle.spai(A, "mgs")
+    m_h, _, _, _ = oracle.spai(A, "householder")
+    m, res, info = ctx.build_h(A)
+    assert info.cols_total == A.n
+    assert info.cols_small + info.cols_large == A.n
+    assert info.cols_singular == sing_o == 0
+    assert rel_err(m, m_h) < RTOL_FP64
+    assert rel_err(m, m_o) < RTOL_FP64
+    assert np.max(np.abs(res - res_o)) < 1e-10
+
+
+def test_schedules_identical(ctx):
+    A = W.circuit_like()
+    m0, r0, _ = ctx.build_h(A, schedule=N.SCHED_BALANCED_COLUMNS)
+    m1, r1, _ = ctx.build_h(A, schedule=N.SCHED_BALANCED_NNZ)
+    assert np.array_equal(m0, m1)
+    assert np.array_equal(r0, r1)
+
+
+def test_column_range_zero_outside(ctx):
+    A = W.convdiff2d(32, 10.0)
+    s, e = 100, 777
+    m, res, info = ctx.build_h(A, col_start=s, col_end=e)
+    m_o, res_o, _, _ = oracle.spai(A, "mgs", s, e)
+    assert info.cols_total == e - s
+    assert rel_err(m, m_o) < RTOL_FP64
+    assert np.all(m[: A.ptr[s]] == 0) and np.all(m[A.ptr[e]:] == 0)
+
+
+def test_spai_fp32(ctx):
+    A = W.convdiff3d(16, 20.0)
+    m_o, _, _, _ = oracle.spai(A, "householder")
+    m, _, info = ctx.build_h(A, precision=N.PREC_MIXED_FP32)
+    assert rel_err(m, m_o) < RTOL_FP32
+
+
+def test_spai_random_unsorted_and_empty(ctx):
+    A = random_csc(300, 0.02, 5, empty_cols=4)
+    m_h, res_h, _, sing = oracle.spai(A, "householder")
+    m, res, info = ctx.build_h(A)
+    ok = np.isfinite(m_h)
+    # columns whose least-squares problem is rank deficient give inf/nan on both sides
+    assert info.cols_singular == sing
+    good_cols = [k for k in range(A.n) if np.all(np.isfinite(m_h[A.ptr[k]:A.ptr[k + 1]]))]
+    for k in good_cols:
+        a, b = m[A.ptr[k]:A.ptr[k + 1]], m_h[A.ptr[k]:A.ptr[k + 1]]
+        if len(b):
+            assert np.max(np.abs(a - b)) <= 1e-8 * max(1.0, np.max(np.abs(b))), k
+    assert ok.sum() > 0
