@@ -1,0 +1,321 @@
+"""Benchmark: SPAI build + BiCGSTAB to 1e-8 relative residual on one B200.
+
+Workload (one "step" = one whole solve): 3D 7-point upwind convection-
+diffusion on a 128^3 grid (n = 2,097,152, nnz = 14,581,760, Pe 20),
+b = A x_true with x_true ~ N(0,1) (seeded), x0 = 0, SPAI pattern = pattern of
+A, BiCGSTAB to ||b - A x|| < 1e-8 ||b|| (verified in FP64), maxiter 1000.
+Synthetic seeded data; the reference publishes no number for it.
+
+  value  ms of the headline form (mixed precision M + FP32 least squares,
+         --form) with A, b resident in HBM
+  e2e    the same through the host-buffer C entry point dcu_spai_solve_h:
+         pinned host A, b, x0 -> device, solve, x -> host, per step
+  plain_fp64_ms  the plain FP64 form on the same inputs (the north star's
+         comparison), measured in the same run
+
+python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Under torchrun each rank solves its own copy (replicas; weak scaling, no
+collective on the data path); ms is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+FORMS = {"fp64": 0, "mixed_fp32": 1, "mixed_bf16": 2, "m_fp32": 3, "m_bf16": 4}
+METRIC = "SPAI build+BiCGSTAB ms to 1e-8 rel. residual (128^3 convection-diffusion)"
+
+
+def workload(m=128, pe=20.0):
+    from dcu_b200 import workloads as W
+
+    A = W.convdiff3d(m, pe)
+    b, xt = W.rhs_from_solution(A, seed=7)
+    return A, b, xt
+
+
+def bytes_per_kernel(n, nnz, w_m, w_v, w_i):
+    """Algorithmic HBM bytes of the five fused iteration kernels (one launch)."""
+    return [
+        nnz * (w_m + w_i) + n * (16 + 3 * w_v),   # K1 p = r + beta(p - w ay), y = M p
+        nnz * (8 + w_i) + n * (8 + 2 * w_v),      # K2 ay = A y, (r*, ay)
+        nnz * (w_m + w_i) + n * (24 + w_v),       # K3 s = r - alpha ay, z = M s
+        nnz * (8 + w_i) + n * (16 + w_v),         # K4 az = A z, (az, s), (az, az)
+        n * (40 + 3 * w_v),                       # K5 x, r update, (r*, r), (r, r)
+    ]
+
+
+def form_widths(form):
+    # (M value bytes, preconditioned-vector bytes, index bytes)
+    return {0: (8, 8, 4), 1: (4, 4, 2), 2: (2, 4, 2), 3: (4, 8, 2), 4: (2, 8, 2)}[form]
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as fh:
+            for line in fh:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference algorithm on the host cores (oracle port)."""
+    if rank != 0:
+        return 0
+    import oracle
+
+    A, b, xt = workload()
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+
+    def step():
+        t0 = time.perf_counter()
+        m, _, _, _ = oracle.spai(A, "mgs")
+        r = oracle.bicgstab(A, m, b, None, tol=1e-8, tol_mode="rel", maxiter=1000)
+        return (time.perf_counter() - t0) * 1e3, r
+
+    for _ in range(args.warmup):
+        step()
+    times, r = [], None
+    for _ in range(args.steps):
+        t, r = step()
+        times.append(t)
+    ms = statistics.mean(times)
+    line = {"impl": "reference", "metric": METRIC, "value": round(ms, 3), "unit": "ms", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "convdiff3d 128^3 Pe 20, b = A x_true, tol 1e-8 rel", "n": A.n, "nnz": A.nnz,
+                       "iters": r["iters"], "rel_res": r["true_res"] / float(np.linalg.norm(b))},
+            "cpu_baseline": {"value": round(ms, 3), "unit": "ms", "cores": threads, "kind": "port",
+                             "sample": "full workload per step (MGS SPAI + BiCGSTAB, C++/OpenMP restatement)"},
+            "e2e": {"value": round(ms, 3), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--form", default="mixed_bf16", choices=list(FORMS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-only", action="store_true", help="one plain + one headline solve, no timing loop")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+
+    from dcu_b200 import native as N
+    from dcu_b200.api import Context
+
+    A, b_h, xt = workload()
+    n, nnz = A.n, A.nnz
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    ptr, idx, val, b = t(A.ptr), t(A.idx), t(A.val), t(b_h)
+    x = torch.zeros(n, dtype=torch.float64, device=dev)
+    mval = torch.zeros(nnz, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > L2 (126 MB)
+    stream = torch.cuda.current_stream(dev)
+    ctx = Context(local)
+    ctx.set_stream(stream.cuda_stream)
+    head = FORMS[args.form]
+
+    def solve(form):
+        x.zero_()
+        return ctx.solve_d(n, nnz, ptr, idx, val, b, x, mval_d=mval, precision=form)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    def timed(form, steps):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        infos = []
+        l0 = ctx.launches
+        for i in range(steps):
+            flush.fill_(float(i))
+            ev[i][0].record(stream)
+            infos.append(solve(form))
+            ev[i][1].record(stream)
+        torch.cuda.synchronize(dev)
+        ms = [a.elapsed_time(z) for a, z in ev]
+        return ms, infos, ctx.launches - l0
+
+    for _ in range(args.warmup):
+        solve(head)
+        solve(FORMS["fp64"])
+    barrier()
+    steps = 1 if args.profile_only else args.steps
+    with Clocks(local) as clk:
+        ms_head, inf_head, launches = timed(head, steps)
+        barrier()
+    clocks = clk.summary()
+    ms_plain, inf_plain, _ = timed(FORMS["fp64"], steps)
+    barrier()
+
+    xh = x.cpu().numpy()  # last plain solve
+    relres_plain = float(np.linalg.norm(b_h - A.matvec(xh)) / np.linalg.norm(b_h))
+    solve(head)
+    torch.cuda.synchronize(dev)
+    xm = x.cpu().numpy()
+    relres_head = float(np.linalg.norm(b_h - A.matvec(xm)) / np.linalg.norm(b_h))
+
+    # per-kernel timing of the headline form's iteration kernels (after its solve)
+    kms = ctx.profile_iteration(reps=20)
+    w_m, w_v, w_i = form_widths(head)
+    kbytes = bytes_per_kernel(n, nnz, w_m, w_v, w_i)
+    j = int(np.argmax(kms))
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = kbytes[j] / (kms[j] * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": ["k_bi_py", "k_bi_ay", "k_bi_sz", "k_bi_az", "k_bi_xr"][j],
+                "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 3),
+                "traffic": None, "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                "kernel_ms": [round(v, 4) for v in kms],
+                "kernel_GBps": [round(kb / (v * 1e-3) / 1e9, 1) for kb, v in zip(kbytes, kms)]}
+
+    # end to end through the host-buffer entry point
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+    hp, hi, hv, hb = pin(A.ptr), pin(A.idx), pin(A.val), pin(b_h)
+    hx = pin(np.zeros(n))
+    e2e_ms = []
+    for i in range(max(1, steps)):
+        hx[:] = 0.0
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ctx.solve_h_into(n, nnz, hp, hi, hv, hb, hx, precision=head)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        e2e_ms.append(e0.elapsed_time(e1))
+    h2d = 4 * (n + 1) + 12 * nnz + 16 * n
+    d2h = 8 * n
+
+    ms = statistics.mean(ms_head)
+    if dist is not None:
+        tt = torch.tensor([ms, statistics.mean(e2e_ms), statistics.mean(ms_plain)], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms, e2e_v, plain_v = [float(v) for v in tt.cpu()]
+    else:
+        e2e_v, plain_v = statistics.mean(e2e_ms), statistics.mean(ms_plain)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.profile_only:
+        import oracle
+
+        threads = os.cpu_count() or 1
+        oracle.set_threads(threads)
+        t0 = time.perf_counter()
+        m_o, _, _, _ = oracle.spai(A, "mgs")
+        r_o = oracle.bicgstab(A, m_o, b_h, None, tol=1e-8, tol_mode="rel", maxiter=1000)
+        cms = (time.perf_counter() - t0) * 1e3
+        cpu = {"value": round(cms, 1), "unit": "ms", "cores": threads, "kind": "port",
+               "sample": f"full 128^3 workload once (MGS SPAI + BiCGSTAB, {r_o['iters']} iterations)"}
+
+    if rank == 0:
+        hi_, pl_ = inf_head[-1], inf_plain[-1]
+        line = {
+            "metric": METRIC, "value": round(ms, 3), "unit": "ms", "n_gpus": world, "steps": steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64+" + args.form, "data": "synthetic",
+            "config": {"workload": "convdiff3d 128^3 Pe 20, b = A x_true, x0 = 0, SPAI(pattern A) + BiCGSTAB "
+                                   "to 1e-8 rel", "n": n, "nnz": nnz, "form": args.form,
+                       "parallelism": f"replicas x{world}" if world > 1 else "single",
+                       "l2": "flushed between steps (256 MB write); A alone is 175 MB > L2",
+                       "iters": hi_[1].iters, "build_ms": round(hi_[0].ms, 3), "solve_ms": round(hi_[1].ms, 3),
+                       "rel_res": relres_head,
+                       "plain_fp64_ms": round(plain_v, 3), "plain_fp64_iters": pl_[1].iters,
+                       "plain_fp64_build_ms": round(pl_[0].ms, 3), "plain_rel_res": relres_plain,
+                       "speedup_vs_plain_fp64": round(plain_v / ms, 3),
+                       "ms_steps": [round(v, 3) for v in ms_head]},
+            "e2e": {"value": round(e2e_v, 3), "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
+            "gpu_launches": int(launches / max(1, steps)),
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -114,6 +114,17 @@ class Context:
                                              _p(mval), C.byref(bi), C.byref(si)))
         return x, mval, bi, si
 
+    def solve_h_into(self, n, nnz, ptr, idx, val, b, x, mval=None, **opt):
+        """dcu_spai_solve_h on caller-owned host arrays used as they are
+        (pinned memory stays pinned); x holds x0 on entry, the solution on exit."""
+        for a, dt in ((ptr, np.int32), (idx, np.int32), (val, np.float64), (b, np.float64), (x, np.float64)):
+            assert a.dtype == dt and a.flags["C_CONTIGUOUS"]
+        o = N.default_options(**opt)
+        bi, si = N.BuildInfo(), N.SolveInfo()
+        self._check(self._L.dcu_spai_solve_h(self.h, n, nnz, _p(ptr), _p(idx), _p(val), _p(b), _p(x), C.byref(o),
+                                             _p(mval), C.byref(bi), C.byref(si)))
+        return bi, si
+
     # ---------------------------------------------------------- device entry
     def pattern_d(self, n, ptr_d, idx_d, col_start=0, col_end=None):
         """(icount, iptr, ilist) as torch tensors on the device."""
@@ -138,6 +149,11 @@ class Context:
         self._check(self._L.dcu_spai_build_d(self.h, n, nnz, _p(ptr_d), _p(idx_d), _p(val_d), C.byref(o),
                                              _p(mval_d), _p(colres_d), C.byref(info)))
         return info
+
+    def profile_iteration(self, reps: int = 20):
+        ms = (C.c_float * 5)()
+        self._check(self._L.dcu_profile_iteration_kernels(self.h, reps, ms))
+        return [float(v) for v in ms]
 
     def csc_to_csr_d(self, n, nnz, ptr_d, idx_d, val_d, rptr_d, ridx_d, rval_d):
         self._check(self._L.dcu_csc_to_csr_d(self.h, n, nnz, _p(ptr_d), _p(idx_d), _p(val_d), _p(rptr_d),

@@ -24,6 +24,8 @@
 //          with exactly the y, z, A y, A z that were stored, so the recurrence
 //          residual tracks b - A x to FP64 rounding.
 #include <cmath>
+#include <algorithm>
+#include <cstddef>
 
 #include "internal.cuh"
 
@@ -377,7 +379,23 @@ template <typename MT, typename IT, typename VT>
 int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval, const IT* ix, const double* b,
                double* x, const dcu_options* opt, dcu_solve_info* info) {
   const int n = plan.n;
-  const int grid = waves_grid(c, n, BI_BLOCK, 2048 / BI_BLOCK);
+  // one full wave per kernel: as many blocks as are resident at once
+  auto gsize = [&](const void* fn) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, BI_BLOCK, 0) != cudaSuccess || per_sm < 1) {
+      cudaGetLastError();
+      per_sm = 1;
+    }
+    return waves_grid(c, n, BI_BLOCK, per_sm);
+  };
+  const int g_init = gsize((const void*)k_bi_init<MT, IT, VT>);
+  const int g_py = gsize((const void*)k_bi_py<MT, IT, VT>);
+  const int g_ay = gsize((const void*)k_bi_ay<MT, IT, VT>);
+  const int g_sz = gsize((const void*)k_bi_sz<MT, IT, VT>);
+  const int g_az = gsize((const void*)k_bi_az<MT, IT, VT>);
+  const int g_xr = gsize((const void*)k_bi_xr<MT, IT, VT>);
+  const int g_tr = gsize((const void*)k_bi_true<MT, IT, VT>);
+  const int grid = std::max({g_init, g_py, g_ay, g_sz, g_az, g_xr, g_tr});  // partial-sum slots
   // vectors: r, ay, s, az (double) + rs, p0, p1, y, z (VT), 256-byte aligned
   auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
   const size_t nd = al(sizeof(double) * (size_t)n), nv = al(sizeof(VT) * (size_t)n);
@@ -407,12 +425,14 @@ int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval,
   DCU_CUDA(c, cudaMemsetAsync(a.S, 0, sizeof(Scal), c->stream));
   int maxiter = opt->maxiter > 0 ? opt->maxiter : n;  // bicgstab_solver.h:134
   DCU_CUDA(c, cudaEventRecord(c->ev[0], c->stream));
-  k_bi_init<MT, IT, VT><<<grid, BI_BLOCK, 0, c->stream>>>(a, opt->tol, opt->tol_mode, maxiter, opt->verify);
+  k_bi_init<MT, IT, VT><<<g_init, BI_BLOCK, 0, c->stream>>>(a, opt->tol, opt->tol_mode, maxiter, opt->verify);
   DCU_LAUNCHED(c, "k_bi_init");
 
   // graph of CHUNK_ITERS iterations
-  std::vector<const void*> key = {plan.off, ix, aval, mval, b, x, base, a.part, a.S, (const void*)(intptr_t)n,
-                                  (const void*)(intptr_t)grid};
+  // the key names the kernel instantiation too: the same buffers are reused
+  // by every precision form
+  std::vector<const void*> key = {(const void*)&k_bi_py<MT, IT, VT>, plan.off, ix, aval, mval, b, x, base, a.part,
+                                  a.S, (const void*)(intptr_t)n, (const void*)(intptr_t)grid};
   GraphSlot* ge = nullptr;
   for (auto& e : c->graphs)
     if (e.key == key) ge = &e;
@@ -420,11 +440,11 @@ int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval,
     cudaGraph_t g = nullptr;
     DCU_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     for (int i = 0; i < CHUNK_ITERS; ++i) {
-      k_bi_py<MT, IT, VT><<<grid, BI_BLOCK, 0, c->stream>>>(a);
-      k_bi_ay<MT, IT, VT><<<grid, BI_BLOCK, 0, c->stream>>>(a);
-      k_bi_sz<MT, IT, VT><<<grid, BI_BLOCK, 0, c->stream>>>(a);
-      k_bi_az<MT, IT, VT><<<grid, BI_BLOCK, 0, c->stream>>>(a);
-      k_bi_xr<MT, IT, VT><<<grid, BI_BLOCK, 0, c->stream>>>(a);
+      k_bi_py<MT, IT, VT><<<g_py, BI_BLOCK, 0, c->stream>>>(a);
+      k_bi_ay<MT, IT, VT><<<g_ay, BI_BLOCK, 0, c->stream>>>(a);
+      k_bi_sz<MT, IT, VT><<<g_sz, BI_BLOCK, 0, c->stream>>>(a);
+      k_bi_az<MT, IT, VT><<<g_az, BI_BLOCK, 0, c->stream>>>(a);
+      k_bi_xr<MT, IT, VT><<<g_xr, BI_BLOCK, 0, c->stream>>>(a);
     }
     cudaError_t e = cudaStreamEndCapture(c->stream, &g);
     if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture", __FILE__, __LINE__);
@@ -445,6 +465,20 @@ int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval,
   // Chunks are launched one ahead of the flag that is read back, so the GPU
   // never idles on the host; after convergence at most one chunk of
   // early-exit kernels runs.
+  c->profile_kernels = 5;
+  c->profile_launch = [c, a, g_py, g_ay, g_sz, g_az, g_xr](int j) -> int {
+    DCU_CUDA(c, cudaMemsetAsync(&a.S->done, 0, sizeof(int), c->stream));
+    switch (j) {
+      case 0: k_bi_py<MT, IT, VT><<<g_py, BI_BLOCK, 0, c->stream>>>(a); break;
+      case 1: k_bi_ay<MT, IT, VT><<<g_ay, BI_BLOCK, 0, c->stream>>>(a); break;
+      case 2: k_bi_sz<MT, IT, VT><<<g_sz, BI_BLOCK, 0, c->stream>>>(a); break;
+      case 3: k_bi_az<MT, IT, VT><<<g_az, BI_BLOCK, 0, c->stream>>>(a); break;
+      default: k_bi_xr<MT, IT, VT><<<g_xr, BI_BLOCK, 0, c->stream>>>(a); break;
+    }
+    DCU_LAUNCHED(c, "profile kernel");
+    return DCU_OK;
+  };
+
   Scal hs;
   Scal* pin = reinterpret_cast<Scal*>(c->pinned);
   int* flag = reinterpret_cast<int*>(reinterpret_cast<char*>(c->pinned) + 1024);
@@ -469,7 +503,7 @@ int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval,
     DCU_CUDA(c, cudaStreamSynchronize(c->stream));
     hs = *pin;
     if (hs.verify_pending) {
-      k_bi_true<MT, IT, VT><<<grid, BI_BLOCK, 0, c->stream>>>(a, 1);
+      k_bi_true<MT, IT, VT><<<g_tr, BI_BLOCK, 0, c->stream>>>(a, 1);
       DCU_LAUNCHED(c, "k_bi_true");
       DCU_CUDA(c, cudaMemcpyAsync(pin, a.S, sizeof(Scal), cudaMemcpyDeviceToHost, c->stream));
       DCU_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -479,7 +513,7 @@ int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval,
     break;
   }
   if (hs.true_res < 0.0) {
-    k_bi_true<MT, IT, VT><<<grid, BI_BLOCK, 0, c->stream>>>(a, 0);
+    k_bi_true<MT, IT, VT><<<g_tr, BI_BLOCK, 0, c->stream>>>(a, 0);
     DCU_LAUNCHED(c, "k_bi_true");
   }
   DCU_CUDA(c, cudaEventRecord(c->ev[1], c->stream));
@@ -504,18 +538,48 @@ int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval,
 
 int bicgstab_solve(Ctx* c, const SellPlan& plan, const double* aval_sell, const void* mval_sell, const double* b,
                    double* x, const dcu_options* opt, dcu_solve_info* info) {
-  if (opt->precision == DCU_PREC_FP64)
+  const int p = opt->precision;
+  if (p == DCU_PREC_FP64)
     return run_solver<double, int, double>(c, plan, aval_sell, (const double*)mval_sell, plan.idx, b, x, opt, info);
-  if (opt->precision == DCU_PREC_MIXED_FP32) {
-    if (plan.delta16)
-      return run_solver<float, int16_t, float>(c, plan, aval_sell, (const float*)mval_sell, plan.del, b, x, opt, info);
-    return run_solver<float, int, float>(c, plan, aval_sell, (const float*)mval_sell, plan.idx, b, x, opt, info);
+  const bool m32 = (p == DCU_PREC_MIXED_FP32 || p == DCU_PREC_M_FP32);
+  const bool v32 = (p == DCU_PREC_MIXED_FP32 || p == DCU_PREC_MIXED_BF16);
+  const float* mf = (const float*)mval_sell;
+  const __nv_bfloat16* mb = (const __nv_bfloat16*)mval_sell;
+  if (plan.delta16) {
+    if (m32) return v32 ? run_solver<float, int16_t, float>(c, plan, aval_sell, mf, plan.del, b, x, opt, info)
+                        : run_solver<float, int16_t, double>(c, plan, aval_sell, mf, plan.del, b, x, opt, info);
+    return v32 ? run_solver<__nv_bfloat16, int16_t, float>(c, plan, aval_sell, mb, plan.del, b, x, opt, info)
+               : run_solver<__nv_bfloat16, int16_t, double>(c, plan, aval_sell, mb, plan.del, b, x, opt, info);
   }
-  if (plan.delta16)
-    return run_solver<__nv_bfloat16, int16_t, float>(c, plan, aval_sell, (const __nv_bfloat16*)mval_sell, plan.del, b,
-                                                     x, opt, info);
-  return run_solver<__nv_bfloat16, int, float>(c, plan, aval_sell, (const __nv_bfloat16*)mval_sell, plan.idx, b, x,
-                                               opt, info);
+  if (m32) return v32 ? run_solver<float, int, float>(c, plan, aval_sell, mf, plan.idx, b, x, opt, info)
+                      : run_solver<float, int, double>(c, plan, aval_sell, mf, plan.idx, b, x, opt, info);
+  return v32 ? run_solver<__nv_bfloat16, int, float>(c, plan, aval_sell, mb, plan.idx, b, x, opt, info)
+             : run_solver<__nv_bfloat16, int, double>(c, plan, aval_sell, mb, plan.idx, b, x, opt, info);
+}
+
+int profile_iteration(Ctx* c, int reps, float* ms) {
+  if (!c->profile_launch) return fail(c, DCU_ERR_ARG, "no solve has run on this context");
+  if (reps < 1) reps = 1;
+  // cost of the stop-flag reset that precedes every launch
+  int* done = reinterpret_cast<int*>(c->buf[B_SCAL].p) + offsetof(Scal, done) / sizeof(int);
+  DCU_CUDA(c, cudaEventRecord(c->ev[0], c->stream));
+  for (int r = 0; r < reps; ++r) DCU_CUDA(c, cudaMemsetAsync(done, 0, sizeof(int), c->stream));
+  DCU_CUDA(c, cudaEventRecord(c->ev[1], c->stream));
+  DCU_CUDA(c, cudaEventSynchronize(c->ev[1]));
+  float reset = 0.f;
+  cudaEventElapsedTime(&reset, c->ev[0], c->ev[1]);
+  reset /= reps;
+  for (int j = 0; j < c->profile_kernels; ++j) {
+    DCU_TRY(c->profile_launch(j));  // warm-up
+    DCU_CUDA(c, cudaEventRecord(c->ev[0], c->stream));
+    for (int r = 0; r < reps; ++r) DCU_TRY(c->profile_launch(j));
+    DCU_CUDA(c, cudaEventRecord(c->ev[1], c->stream));
+    DCU_CUDA(c, cudaEventSynchronize(c->ev[1]));
+    float t = 0.f;
+    cudaEventElapsedTime(&t, c->ev[0], c->ev[1]);
+    ms[j] = t / reps - reset;
+  }
+  return DCU_OK;
 }
 
 void release_graphs(Ctx* c) {

@@ -45,7 +45,7 @@ int resolve_range(Ctx* c, int n, const dcu_options* in, dcu_options* out) {
     return dcu::fail(c, DCU_ERR_ARG, "invalid column range [%d, %d) for n = %d", out->col_start, out->col_end, n);
   if (out->schedule != DCU_SCHED_BALANCED_COLUMNS && out->schedule != DCU_SCHED_BALANCED_NNZ)
     return dcu::fail(c, DCU_ERR_ARG, "unknown schedule %d", out->schedule);
-  if (out->precision < DCU_PREC_FP64 || out->precision > DCU_PREC_MIXED_BF16)
+  if (out->precision < DCU_PREC_FP64 || out->precision > DCU_PREC_M_BF16)
     return dcu::fail(c, DCU_ERR_ARG, "unknown precision %d", out->precision);
   if (out->tol_mode != DCU_TOL_ABS && out->tol_mode != DCU_TOL_REL)
     return dcu::fail(c, DCU_ERR_ARG, "unknown tolerance mode %d", out->tol_mode);
@@ -63,7 +63,7 @@ int prepare_solve(Ctx* c, int n, int nnz, const int* ptr, const int* idx, const 
   if (precision == DCU_PREC_FP64) {
     DCU_TRY(dcu::ensure(c, dcu::B_SELL_MVAL, sizeof(double) * slots));
     DCU_TRY(dcu::sell_gather_f64(c, *plan, mval, dcu::bp<double>(c, dcu::B_SELL_MVAL)));
-  } else if (precision == DCU_PREC_MIXED_FP32) {
+  } else if (precision == DCU_PREC_MIXED_FP32 || precision == DCU_PREC_M_FP32) {
     DCU_TRY(dcu::ensure(c, dcu::B_SELL_MVAL, sizeof(float) * slots));
     DCU_TRY(dcu::sell_gather_f32(c, *plan, mval, dcu::bp<float>(c, dcu::B_SELL_MVAL)));
   } else {
@@ -155,8 +155,9 @@ int dcu_spai_create(dcu_spai_ctx** out, int device, int units) {
     dcu_spai_destroy(c);
     return rc;
   }
-  // the schedules split columns over the small kernel's 8-lane groups
-  c->units = units > 0 ? units : c->sms * 4 * 16;
+  // the static schedule splits columns over `units` ranges; by default one
+  // per resident warp of the column kernel
+  c->units = units > 0 ? units : dcu::spai_default_units(c);
   *out = c;
   return DCU_OK;
 }
@@ -372,6 +373,12 @@ int dcu_spai_solve_d(dcu_spai_ctx* c, int n, int nnz, const int* ptr, const int*
   } catch (const std::bad_alloc&) {
     return dcu::fail(c, DCU_ERR_ALLOC, "host allocation failed");
   }
+}
+
+int dcu_profile_iteration_kernels(dcu_spai_ctx* c, int reps, float* ms_out) {
+  if (!c || !ms_out) return DCU_ERR_ARG;
+  StreamScope scope(c);
+  return dcu::profile_iteration(c, reps, ms_out);
 }
 
 int dcu_spai_solve_h(dcu_spai_ctx* c, int n, int nnz, const int* ptr, const int* idx, const double* val,

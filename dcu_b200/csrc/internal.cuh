@@ -7,6 +7,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -72,6 +73,10 @@ struct Ctx {
   void* pinned = nullptr;   // small pinned host scratch (flags, stats), kPinnedBytes
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   std::vector<GraphSlot> graphs;  // BiCGSTAB iteration graphs (bounded cache)
+  // launches iteration kernel j (0..4) of the last solve on its buffers, with
+  // the solver's stop flag cleared first (diagnostic timing only)
+  std::function<int(int)> profile_launch;
+  int profile_kernels = 0;
 };
 
 constexpr size_t kPinnedBytes = 4096;
@@ -141,6 +146,9 @@ int sell_gather_bf16(Ctx* c, const SellPlan& p, const double* src, __nv_bfloat16
 // ---------------------------------------------------------------------------
 int spai_build(Ctx* c, int n, int nnz, const int* ptr, const int* idx, const double* val,
                const dcu_options* opt, double* mval, double* colres, dcu_build_info* info);
+// Work units of the static schedule when the caller names none: one per
+// resident warp of the column kernel.
+int spai_default_units(Ctx* c);
 int spai_pattern(Ctx* c, int n, const int* ptr, const int* idx, int col_start, int col_end,
                  int* icount, long long* iptr, int* ilist, long long cap, long long* total);
 
@@ -150,6 +158,7 @@ int spai_pattern(Ctx* c, int n, const int* ptr, const int* idx, int col_start, i
 int bicgstab_solve(Ctx* c, const SellPlan& plan, const double* aval_sell, const void* mval_sell,
                    const double* b, double* x, const dcu_options* opt, dcu_solve_info* info);
 void release_graphs(Ctx* c);
+int profile_iteration(Ctx* c, int reps, float* ms);
 
 // grid size for grid-stride kernels: whole waves of `per_sm` blocks
 inline int waves_grid(const Ctx* c, long long work_items, int block, int per_sm) {

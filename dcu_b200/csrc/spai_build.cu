@@ -49,12 +49,14 @@ enum {
   ST_AREA64 = 7       // long long index (ints 14-15): max candidates * (|J|+1) over queued columns
 };
 
-constexpr int GL = 8;          // lanes per column group
-constexpr int SM_MMAX = 32;    // max |I_k| on the small path
-constexpr int SM_CMAX = 64;    // max candidate rows on the small path
-constexpr int SM_NJMAX = 7;    // max |J_k| on the small path ([At | e] fits 8 lanes)
-constexpr int SM_BLOCK = 128;   // 16 groups: the FP64 group state stays under 48 KB
-constexpr int SM_GROUPS = SM_BLOCK / GL;
+constexpr int GL = 16;          // lanes per least-squares problem: 2 per column of [At | e_E]
+constexpr int SG_GPW = 2;       // problems (groups) per warp
+constexpr int SG_BLOCK = 64;    // 2 warps, 4 groups
+constexpr int SG_WARPS = SG_BLOCK / 32;
+constexpr int SG_MMAX = 32;     // max |I_k| on the group path
+constexpr int SG_CMAX = 64;     // max candidate rows on the group path
+constexpr int SG_NJMAX = 7;     // max |J_k| ([At | e_E] has <= 8 columns)
+constexpr int SG_COLS = 8;
 constexpr unsigned kPad = 0xFFFFFFFFu;
 
 struct SmallArgs {
@@ -64,7 +66,8 @@ struct SmallArgs {
   const double* val;
   int col_start, col_end;
   int schedule;
-  const int* chunks;
+  int units;          // static schedule: balanced_columns split into `units` ranges
+  const int* chunks;  // dynamic schedule: nnz-balanced chunk bounds
   int nchunks;
   double* mval;
   double* colres;
@@ -75,14 +78,17 @@ struct SmallArgs {
   int* stats;
 };
 
+// Shared state of the two groups of a warp.  Row strides are padded so the
+// groups' broadcasts of v fall in different banks.
 template <typename T>
-struct SmallGroup {
-  T At[GL][SM_MMAX];     // column j of [A(I,J) | e_E]; later R and x
-  T v[SM_MMAX];          // Householder vector, then y = Q^T e_E, then x
-  unsigned key[SM_CMAX]; // candidate keys (row << 6 | candidate)
-  int src[SM_CMAX];      // candidate -> position in A's arrays
-  signed char jj[SM_CMAX];
-  T beta;
+struct WarpSmem {
+  T At[SG_GPW][SG_COLS][SG_MMAX + 1];  // column j of [A(I,J) | e_E]; later R
+  T v[SG_GPW][SG_MMAX + 2];            // Householder vector; then y; then x
+  T dinv[SG_GPW][SG_COLS];             // 1 / R_jj
+  T beta[SG_GPW][2];
+  unsigned key[SG_GPW][SG_CMAX];       // candidate keys (row << 6 | candidate)
+  int src[SG_GPW][SG_CMAX];            // candidate -> position in A's arrays
+  signed char jj[SG_GPW][SG_CMAX];
 };
 
 __device__ __forceinline__ void queue_big(const SmallArgs& a, int k, int nj, long long area) {
@@ -92,8 +98,8 @@ __device__ __forceinline__ void queue_big(const SmallArgs& a, int k, int nj, lon
   atomicMax(reinterpret_cast<unsigned long long*>(a.stats) + ST_AREA64, (unsigned long long)area);
 }
 
-// Bitonic sort of 8*PER keys held PER per lane (element e = lane*PER + s),
-// ascending, across the 8 lanes of a group.
+// Bitonic sort of GL*PER keys held PER per lane (element e = lane*PER + s),
+// ascending, across the GL lanes of a group.
 template <int PER>
 __device__ __forceinline__ void group_sort(unsigned (&key)[PER], int lane, unsigned gmask) {
   constexpr int N = GL * PER;
@@ -105,7 +111,7 @@ __device__ __forceinline__ void group_sort(unsigned (&key)[PER], int lane, unsig
         const int lx = jj / PER;
 #pragma unroll
         for (int s = 0; s < PER; ++s) {
-          unsigned other = __shfl_xor_sync(gmask, key[s], lx, GL);
+          const unsigned other = __shfl_xor_sync(gmask, key[s], lx, GL);
           const int e = lane * PER + s;
           const bool up = (e & kk) == 0;
           const bool lower = (e & jj) == 0;
@@ -120,9 +126,9 @@ __device__ __forceinline__ void group_sort(unsigned (&key)[PER], int lane, unsig
             const int e = lane * PER + s;
             const bool up = (e & kk) == 0;
             const unsigned x = key[s], y = key[p];
-            const bool swap = up ? (x > y) : (x < y);
-            key[s] = swap ? y : x;
-            key[p] = swap ? x : y;
+            const unsigned lo = min(x, y), hi = max(x, y);
+            key[s] = up ? lo : hi;
+            key[p] = up ? hi : lo;
           }
         }
       }
@@ -130,20 +136,123 @@ __device__ __forceinline__ void group_sort(unsigned (&key)[PER], int lane, unsig
   }
 }
 
+// Householder QR of [At | e_E] and back substitution.  Lane = 2 * column +
+// half: each lane holds RPL = MMAX / 2 consecutive rows of one column in
+// registers.  The step loop is fully unrolled (steps < 8 <= RPL, so the
+// diagonal entry of every step lives in the first half).  Rows above the step
+// are excluded from the reflector by zeros in v.  Returns true for a zero /
+// non-finite pivot.
+template <int MMAX, typename T>
+__device__ __forceinline__ bool group_qr_solve(const SmallArgs& a, WarpSmem<T>& ws, int g, int lane,
+                                               unsigned gmask, int k, int cs, int nj, int m) {
+  constexpr int RPL = MMAX / 2;
+  const int j = lane >> 1, h = lane & 1, row0 = h * RPL;
+  T r[RPL];
+#pragma unroll
+  for (int t = 0; t < RPL; ++t) r[t] = ws.At[g][j][row0 + t];
+  T* v = ws.v[g];
+  bool sing = false;
+  const int steps = min(nj, m);
+#pragma unroll
+  for (int c = 0; c < SG_NJMAX; ++c) {
+    if (c >= steps) break;
+    // both lanes of column c: norm of rows >= c, reflector, R_cc
+    T part = T(0);
+#pragma unroll
+    for (int t = 0; t < RPL; ++t) part += (row0 + t >= c) ? r[t] * r[t] : T(0);
+    part += __shfl_xor_sync(gmask, part, 1, GL);
+    const T nrm2 = __shfl_sync(gmask, part, 2 * c, GL);
+    const T x0 = __shfl_sync(gmask, r[c], 2 * c, GL);  // row c < RPL: first half
+    const T nrm = sqrt(nrm2);
+    T alpha = T(0), beta = T(0);
+    if (nrm > T(0)) {
+      alpha = (x0 > T(0)) ? -nrm : nrm;
+      beta = T(1) / (nrm * (nrm + fabs(x0)));  // 2 / (v^T v)
+    } else {
+      sing = true;
+    }
+    if (j == c) {
+#pragma unroll
+      for (int t = 0; t < RPL; ++t) {
+        const int i = row0 + t;
+        v[i] = (i < c) ? T(0) : ((i == c) ? x0 - alpha : r[t]);
+        if (i == c) r[t] = alpha;
+        else if (i > c) r[t] = T(0);
+      }
+    }
+    __syncwarp(gmask);
+    const bool trailing = (j > c) && (j <= nj);
+    // v is re-read from shared memory in both loops (volatile) rather than
+    // held in RPL more registers: fewer registers, more resident problems
+    const volatile T* vv = v + row0;
+    T w0 = T(0), w1 = T(0);
+    if (trailing) {
+#pragma unroll
+      for (int t = 0; t < RPL; ++t) {
+        if (t & 1) w1 += vv[t] * r[t];
+        else w0 += vv[t] * r[t];
+      }
+    }
+    T w = w0 + w1;
+    w += __shfl_xor_sync(gmask, w, 1, GL);
+    if (trailing) {
+      w *= beta;
+#pragma unroll
+      for (int t = 0; t < RPL; ++t) r[t] -= w * vv[t];
+    }
+    __syncwarp(gmask);
+  }
+  // R -> At (rows <= column), y -> v, 1/R_jj -> dinv, ||(Q^T e_E)[nj:]||^2
+  T res2 = T(0);
+  if (j < nj && h == 0) {
+    T d = T(0);
+#pragma unroll
+    for (int t = 0; t < SG_COLS; ++t) {
+      if (t <= j) ws.At[g][j][t] = r[t];
+      if (t == j) d = r[t];
+    }
+    if (!(d != T(0)) || !isfinite((double)d)) sing = true;
+    ws.dinv[g][j] = T(1) / d;
+  } else if (j == nj) {
+#pragma unroll
+    for (int t = 0; t < RPL; ++t) {
+      const int i = row0 + t;
+      if (i < nj) v[i] = r[t];
+      else res2 += r[t] * r[t];
+    }
+  }
+  res2 += __shfl_xor_sync(gmask, res2, 1, GL);
+  __syncwarp(gmask);
+  if (lane == 0) {
+    for (int i = nj - 1; i >= 0; --i) {
+      T xi = v[i];
+      for (int jc = i + 1; jc < nj; ++jc) xi -= ws.At[g][jc][i] * v[jc];
+      v[i] = xi * ws.dinv[g][i];
+    }
+  }
+  __syncwarp(gmask);
+  if (lane < nj) a.mval[cs + lane] = (double)v[lane];
+  if (j == nj && h == 0 && a.colres) a.colres[k - a.col_start] = sqrt((double)res2);
+  const unsigned any_sing = __ballot_sync(gmask, sing) & gmask;
+  __syncwarp(gmask);
+  return any_sing != 0;
+}
+
 // Everything after candidate staging for one column, PER keys per lane.
 // Returns |I_k| (or -1 when the column was queued for the CTA kernel).
 template <int PER, typename T, int MODE>
-__device__ __forceinline__ int small_column(const SmallArgs& a, SmallGroup<T>& sg, int k, int cs, int nj, int cand,
-                                            int lane, unsigned gmask) {
+__device__ __forceinline__ int group_column(const SmallArgs& a, WarpSmem<T>& ws, int g, int k, int cs, int nj,
+                                            int cand, int lane, unsigned gmask) {
   unsigned key[PER];
 #pragma unroll
   for (int s = 0; s < PER; ++s) {
     const int t = lane * PER + s;
-    key[s] = (t < cand) ? sg.key[t] : kPad;
+    key[s] = (t < cand) ? ws.key[g][t] : kPad;
   }
   group_sort<PER>(key, lane, gmask);
 
-  // distinct rows: flag the first element of each run of equal rows
+  // distinct rows: flag the first element of each run of equal rows; pre[s]
+  // is the inclusive count of firsts in this lane, negated for repeats
   const unsigned prev = __shfl_up_sync(gmask, key[PER - 1], 1, GL);
   int pre[PER];
   int cnt = 0;
@@ -153,7 +262,7 @@ __device__ __forceinline__ int small_column(const SmallArgs& a, SmallGroup<T>& s
     const unsigned before = (s == 0) ? prev : key[s - 1];
     const bool first = valid && ((s == 0 && lane == 0) || (before >> 6) != (key[s] >> 6));
     cnt += first ? 1 : 0;
-    pre[s] = first ? cnt : -cnt;  // sign marks "first", magnitude = inclusive count
+    pre[s] = first ? cnt : -cnt;
   }
   int inc = cnt;
 #pragma unroll
@@ -164,7 +273,7 @@ __device__ __forceinline__ int small_column(const SmallArgs& a, SmallGroup<T>& s
   const int excl = inc - cnt;
   const int m = __shfl_sync(gmask, inc, GL - 1, GL);
 
-  if (m > SM_MMAX) {
+  if (m > SG_MMAX) {
     if (lane == 0) queue_big(a, k, nj, (long long)cand * (nj + 1));
     return -1;
   }
@@ -188,106 +297,33 @@ __device__ __forceinline__ int small_column(const SmallArgs& a, SmallGroup<T>& s
     if (pre[s] > 0 && (int)(key[s] >> 6) == k) E = excl + pre[s] - 1;
 #pragma unroll
   for (int d = 1; d < GL; d <<= 1) E = max(E, __shfl_xor_sync(gmask, E, d, GL));
-#pragma unroll
-  for (int i = 0; i < SM_MMAX; ++i) sg.At[lane][i] = T(0);
+  for (int i = lane; i < SG_COLS * (SG_MMAX + 1); i += GL) (&ws.At[g][0][0])[i] = T(0);
   __syncwarp(gmask);
 #pragma unroll
   for (int s = 0; s < PER; ++s) {
     if (key[s] != kPad) {
       const int t = key[s] & 63;
       const int pos = excl + (pre[s] > 0 ? pre[s] : -pre[s]) - 1;
-      sg.At[sg.jj[t]][pos] = (T)__ldg(a.val + sg.src[t]);
+      ws.At[g][ws.jj[g][t]][pos] = (T)__ldg(a.val + ws.src[g][t]);
     }
   }
-  if (lane == 0 && E >= 0) sg.At[nj][E] = T(1);
+  if (lane == 0 && E >= 0) ws.At[g][nj][E] = T(1);
   __syncwarp(gmask);
-
-  // ---- Householder QR of [At | e_E]: lane j owns column j ---------------
-  T r[SM_MMAX];
-#pragma unroll
-  for (int i = 0; i < SM_MMAX; ++i) r[i] = sg.At[lane][i];
-  bool sing = m < nj;
-  const int steps = min(nj, m);
-  for (int c = 0; c < steps; ++c) {
-    if (lane == c) {
-      T nrm2 = T(0), x0 = T(0);
-#pragma unroll
-      for (int i = 0; i < SM_MMAX; ++i) {
-        if (i >= c) {
-          nrm2 += r[i] * r[i];
-          sg.v[i] = r[i];
-        }
-        if (i == c) x0 = r[i];
-      }
-      const T nrm = sqrt(nrm2);
-      T alpha = T(0), beta = T(0);
-      if (nrm > T(0)) {
-        alpha = (x0 > T(0)) ? -nrm : nrm;
-        beta = T(1) / (nrm * (nrm + fabs(x0)));  // 2 / (v^T v)
-        sg.v[c] = x0 - alpha;
-      } else {
-        sing = true;
-      }
-      sg.beta = beta;
-#pragma unroll
-      for (int i = 0; i < SM_MMAX; ++i) {
-        if (i == c) r[i] = alpha;
-        else if (i > c) r[i] = T(0);
-      }
-    }
-    __syncwarp(gmask);
-    if (lane > c && lane <= nj) {
-      const T beta = sg.beta;
-      T w = T(0);
-#pragma unroll
-      for (int i = 0; i < SM_MMAX; ++i)
-        if (i >= c) w += sg.v[i] * r[i];
-      w *= beta;
-#pragma unroll
-      for (int i = 0; i < SM_MMAX; ++i)
-        if (i >= c) r[i] -= w * sg.v[i];
-    }
-    __syncwarp(gmask);
-  }
-  // ---- back substitution R x = (Q^T e_E)[0:nj] ---------------------------
-  T res2 = T(0);
-  if (lane < nj) {
-#pragma unroll
-    for (int i = 0; i <= SM_NJMAX; ++i)
-      if (i <= lane) sg.At[lane][i] = r[i];
-  } else if (lane == nj) {
-#pragma unroll
-    for (int i = 0; i < SM_MMAX; ++i) {
-      if (i < nj) sg.v[i] = r[i];
-      else res2 += r[i] * r[i];
-    }
-  }
-  __syncwarp(gmask);
-  if (lane == 0) {
-    for (int i = nj - 1; i >= 0; --i) {
-      T xi = sg.v[i];
-      for (int j = i + 1; j < nj; ++j) xi -= sg.At[j][i] * sg.v[j];
-      const T rii = sg.At[i][i];
-      if (!(rii != T(0)) || !isfinite((double)rii)) sing = true;
-      sg.v[i] = xi / rii;
-    }
-    if (sing) atomicAdd(&a.stats[ST_SINGULAR], 1);
-  }
-  __syncwarp(gmask);
-  if (lane < nj) a.mval[cs + lane] = (double)sg.v[lane];
-  if (lane == nj && a.colres) a.colres[col] = sqrt((double)res2);
-  __syncwarp(gmask);
+  const bool sing = (m < nj) | ((m <= 16) ? group_qr_solve<16, T>(a, ws, g, lane, gmask, k, cs, nj, m)
+                                          : group_qr_solve<32, T>(a, ws, g, lane, gmask, k, cs, nj, m));
+  if (sing && lane == 0) atomicAdd(&a.stats[ST_SINGULAR], 1);
   return m;
 }
 
 template <typename T, int MODE>
-__global__ void __launch_bounds__(SM_BLOCK, 4) k_spai_small(SmallArgs a) {
-  __shared__ SmallGroup<T> groups[SM_GROUPS];
+__global__ void __launch_bounds__(SG_BLOCK) k_spai_small(SmallArgs a) {
+  __shared__ WarpSmem<T> smem[SG_WARPS];
   const int lane = threadIdx.x & (GL - 1);
-  const unsigned gmask = 0xFFu << (threadIdx.x & 24);
-  SmallGroup<T>& sg = groups[threadIdx.x / GL];
-  const int gid = (blockIdx.x * SM_BLOCK + threadIdx.x) / GL;
-  const int ngroups = (gridDim.x * SM_BLOCK) / GL;
+  const int g = (threadIdx.x / GL) & (SG_GPW - 1);
+  const unsigned gmask = 0xFFFFu << (threadIdx.x & 16);
+  WarpSmem<T>& ws = smem[threadIdx.x >> 5];
+  const int gid = (blockIdx.x * SG_BLOCK + threadIdx.x) / GL;
+  const int ngroups = (gridDim.x * SG_BLOCK) / GL;
   int my_max_ni = 0, my_max_nj = 0, my_cols = 0;
 
   auto process = [&](int k) {
@@ -302,7 +338,7 @@ __global__ void __launch_bounds__(SM_BLOCK, 4) k_spai_small(SmallArgs a) {
       ++my_cols;
       return;
     }
-    if (nj > SM_NJMAX) {
+    if (nj > SG_NJMAX) {
       // candidate count is only needed as a slab bound: count it here
       long long cand = 0;
       for (int t = lane; t < nj; t += GL) {
@@ -328,7 +364,7 @@ __global__ void __launch_bounds__(SM_BLOCK, 4) k_spai_small(SmallArgs a) {
     }
     const int cand = __shfl_sync(gmask, inc, GL - 1, GL);
     const int cb = inc - lj;
-    if (cand > SM_CMAX) {
+    if (cand > SG_CMAX) {
       if (lane == 0) queue_big(a, k, nj, (long long)cand * (nj + 1));
       return;
     }
@@ -339,14 +375,15 @@ __global__ void __launch_bounds__(SM_BLOCK, 4) k_spai_small(SmallArgs a) {
       for (int q = lane; q < ljj; q += GL) {
         const int t = cbj + q;
         const int row = __ldg(a.idx + bjj + q);
-        sg.key[t] = ((unsigned)row << 6) | (unsigned)t;
-        sg.src[t] = bjj + q;
-        sg.jj[t] = (signed char)j;
+        ws.key[g][t] = ((unsigned)row << 6) | (unsigned)t;
+        ws.src[g][t] = bjj + q;
+        ws.jj[g][t] = (signed char)j;
       }
     }
     __syncwarp(gmask);
-    const int m = (cand <= 32) ? small_column<4, T, MODE>(a, sg, k, cs, nj, cand, lane, gmask)
-                               : small_column<8, T, MODE>(a, sg, k, cs, nj, cand, lane, gmask);
+    const int m = (cand <= 32) ? group_column<2, T, MODE>(a, ws, g, k, cs, nj, cand, lane, gmask)
+                               : group_column<4, T, MODE>(a, ws, g, k, cs, nj, cand, lane, gmask);
+    __syncwarp(gmask);
     if (m >= 0) {
       my_max_ni = max(my_max_ni, m);
       ++my_cols;
@@ -354,12 +391,15 @@ __global__ void __launch_bounds__(SM_BLOCK, 4) k_spai_small(SmallArgs a) {
   };
 
   if (a.schedule == DCU_SCHED_BALANCED_COLUMNS) {
-    // unit gid owns a contiguous balanced_columns range
+    // balanced_columns over `units` contiguous ranges; group q takes units
+    // q, q + ngroups, ...
     const int total = a.col_end - a.col_start;
-    const int base = total / ngroups, rem = total % ngroups;
-    const int start = a.col_start + gid * base + min(gid, rem);
-    const int end = start + base + (gid < rem ? 1 : 0);
-    for (int k = start; k < end; ++k) process(k);
+    const int base = total / a.units, rem = total % a.units;
+    for (int u = gid; u < a.units; u += ngroups) {
+      const int start = a.col_start + u * base + min(u, rem);
+      const int end = start + base + (u < rem ? 1 : 0);
+      for (int k = start; k < end; ++k) process(k);
+    }
   } else {
     // nnz-balanced chunks pulled from the queue
     for (;;) {
@@ -685,8 +725,26 @@ __global__ void k_nnz_chunks(const int* __restrict__ ptr, int col_start, int col
 }
 
 template <typename T, int MODE>
-int run_small(Ctx* c, const SmallArgs& a, int grid) {
-  k_spai_small<T, MODE><<<grid, SM_BLOCK, 0, c->stream>>>(a);
+int run_small(Ctx* c, SmallArgs a, int) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spai_small<T, MODE>, SG_BLOCK, 0) != cudaSuccess ||
+      per_sm < 1) {
+    cudaGetLastError();
+    per_sm = 1;
+  }
+  const int grid = c->sms * per_sm;
+  const int ngroups = grid * SG_BLOCK / GL;
+  if (a.units <= 0) a.units = ngroups;
+  if (a.schedule == DCU_SCHED_BALANCED_NNZ) {
+    const int nchunks = ngroups * 4;
+    DCU_TRY(ensure(c, B_CHUNKS, sizeof(int) * (size_t)(nchunks + 1)));
+    int* bounds = bp<int>(c, B_CHUNKS);
+    k_nnz_chunks<<<(nchunks + 256) / 256, 256, 0, c->stream>>>(a.ptr, a.col_start, a.col_end, nchunks, bounds);
+    DCU_LAUNCHED(c, "k_nnz_chunks");
+    a.chunks = bounds;
+    a.nchunks = nchunks;
+  }
+  k_spai_small<T, MODE><<<grid, SG_BLOCK, 0, c->stream>>>(a);
   DCU_LAUNCHED(c, "k_spai_small");
   return DCU_OK;
 }
@@ -725,8 +783,7 @@ int prepare(Ctx* c, int n, const int* ptr, const int* idx, const double* val, in
   DCU_TRY(ensure(c, B_BIGLIST, sizeof(int) * (size_t)(ncols > 0 ? ncols : 1)));
   int* stats = bp<int>(c, B_STATS);
   DCU_CUDA(c, cudaMemsetAsync(stats, 0, sizeof(int) * ST_INTS, c->stream));
-  P->grid = c->sms * 4;
-  const int ngroups = P->grid * SM_GROUPS;
+  P->grid = 0;
   SmallArgs& a = P->sa;
   a = SmallArgs{};
   a.n = n;
@@ -738,15 +795,7 @@ int prepare(Ctx* c, int n, const int* ptr, const int* idx, const double* val, in
   a.schedule = schedule;
   a.big_list = bp<int>(c, B_BIGLIST);
   a.stats = stats;
-  if (schedule == DCU_SCHED_BALANCED_NNZ) {
-    const int nchunks = ngroups * 4;
-    DCU_TRY(ensure(c, B_CHUNKS, sizeof(int) * (size_t)(nchunks + 1)));
-    int* bounds = bp<int>(c, B_CHUNKS);
-    k_nnz_chunks<<<(nchunks + 256) / 256, 256, 0, c->stream>>>(ptr, col_start, col_end, nchunks, bounds);
-    DCU_LAUNCHED(c, "k_nnz_chunks");
-    a.chunks = bounds;
-    a.nchunks = nchunks;
-  }
+  a.units = c->units;
   P->stats = stats;
   return DCU_OK;
 }
@@ -802,6 +851,17 @@ int build_typed(Ctx* c, int n, const int* ptr, const int* idx, const double* val
 }
 
 }  // namespace
+
+int spai_default_units(Ctx* c) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spai_small<double, MODE_BUILD>, SG_BLOCK, 0) !=
+          cudaSuccess ||
+      per_sm < 1) {
+    cudaGetLastError();
+    per_sm = 1;
+  }
+  return c->sms * per_sm * (SG_BLOCK / GL);
+}
 
 int spai_build(Ctx* c, int n, int nnz, const int* ptr, const int* idx, const double* val, const dcu_options* opt,
                double* mval, double* colres, dcu_build_info* info) {

@@ -17,7 +17,7 @@ OK, ERR_ARG, ERR_CUDA, ERR_ALLOC, ERR_NO_DEVICE, ERR_LIMIT = range(6)
 # dcu_schedule
 SCHED_BALANCED_COLUMNS, SCHED_BALANCED_NNZ = 0, 1
 # dcu_precision
-PREC_FP64, PREC_MIXED_FP32, PREC_MIXED_BF16 = 0, 1, 2
+PREC_FP64, PREC_MIXED_FP32, PREC_MIXED_BF16, PREC_M_FP32, PREC_M_BF16 = 0, 1, 2, 3, 4
 # dcu_tol_mode
 TOL_ABS, TOL_REL = 0, 1
 # dcu_solve_status
@@ -64,6 +64,7 @@ SIGNATURES = {
                               C.POINTER(SolveInfo)]),
     "dcu_spai_solve_h": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _OPT, _vp, C.POINTER(BuildInfo),
                               C.POINTER(SolveInfo)]),
+    "dcu_profile_iteration_kernels": (_i, [_vp, _i, C.POINTER(C.c_float)]),
     "dcu_mtx_read": (_i, [C.c_char_p, C.POINTER(_i), C.POINTER(_i), C.POINTER(C.POINTER(_i)),
                           C.POINTER(C.POINTER(_i)), C.POINTER(C.POINTER(C.c_double))]),
     "dcu_mtx_free": (None, [_vp]),

@@ -62,7 +62,9 @@ typedef enum {
   DCU_PREC_FP64 = 0,      /* plain: FP64 least squares, FP64 M, FP64 vectors, int32 indices */
   DCU_PREC_MIXED_FP32 = 1,/* FP32 least squares, M stored FP32, FP32 preconditioned vectors,
                              16-bit index deltas where they fit; FP64 A, residual, dots   */
-  DCU_PREC_MIXED_BF16 = 2 /* as MIXED_FP32 with M stored as BF16                           */
+  DCU_PREC_MIXED_BF16 = 2,/* as MIXED_FP32 with M stored as BF16                           */
+  DCU_PREC_M_FP32 = 3,    /* FP32 least squares and M (FP32, 16-bit deltas); every vector FP64 */
+  DCU_PREC_M_BF16 = 4     /* as M_FP32 with M stored as BF16                               */
 } dcu_precision;
 
 /* Stopping rule. */
@@ -118,8 +120,9 @@ void dcu_options_default(dcu_options* opt);
 /* ---- context ------------------------------------------------------------- */
 
 /* Create a context on CUDA device `device`.  `units` is the schedule's unit
- * count P (the reference's numDCUs); <= 0 picks 4 warp-groups per resident
- * warp slot of the device.  Replaces initMultiDCU. */
+ * count P (the reference's numDCUs): balanced_columns splits the columns into
+ * P contiguous ranges that the resident warps take in turn; <= 0 picks one
+ * unit per resident warp of the column kernel.  Replaces initMultiDCU. */
 int dcu_spai_create(dcu_spai_ctx** ctx, int device, int units);
 /* Frees every device buffer the context owns.  Replaces cleanupMultiDCU. */
 void dcu_spai_destroy(dcu_spai_ctx* ctx);
@@ -190,6 +193,13 @@ int dcu_spai_solve_d(dcu_spai_ctx* ctx, int n, int nnz, const int* ptr, const in
 int dcu_spai_solve_h(dcu_spai_ctx* ctx, int n, int nnz, const int* ptr, const int* idx,
                      const double* val, const double* b, double* x, const dcu_options* opt,
                      double* mval, dcu_build_info* binfo, dcu_solve_info* sinfo);
+
+/* Diagnostic timing: re-launch each of the five fused iteration kernels of
+ * the last solve on this context (K1 p/y = M p, K2 A y + (r*,Ay), K3 s/z = M s,
+ * K4 A z + dots, K5 x/r update + dots) `reps` times on that solve's buffers
+ * and write the mean device time per launch (ms) to ms_out[0..4].  The
+ * solver vectors and x are left in an unspecified state. */
+int dcu_profile_iteration_kernels(dcu_spai_ctx* ctx, int reps, float* ms_out);
 
 /* ---- MatrixMarket input (command-line driver) --------------------------------- */
 

@@ -22,7 +22,7 @@ def test_config1_reference_settings(ctx):
     assert info.res < 1e-7
 
 
-@pytest.mark.parametrize("prec", [N.PREC_FP64, N.PREC_MIXED_FP32, N.PREC_MIXED_BF16])
+@pytest.mark.parametrize("prec", [N.PREC_FP64, N.PREC_MIXED_FP32, N.PREC_MIXED_BF16, N.PREC_M_FP32, N.PREC_M_BF16])
 def test_config1_solve(ctx, prec):
     A = W.convdiff2d(64, 10.0)
     b = W.rhs_ones_product(A)
@@ -36,7 +36,9 @@ def test_config1_solve(ctx, prec):
     if prec == N.PREC_FP64:
         assert abs(si.iters - ref["iters"]) <= 1
     else:
-        assert abs(si.iters - ref["iters"]) <= max(3, ref["iters"] // 10)
+        # a different (rounded) preconditioner / FP32 Krylov vectors: the
+        # count may move, the verified residual may not
+        assert si.iters <= 1.25 * ref["iters"] + 3
     assert np.max(np.abs(x - 1.0)) < 1e-5
 
 

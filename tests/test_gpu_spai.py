@@ -73,3 +73,15 @@ def test_spai_random_unsorted_and_empty(ctx):
         if len(b):
             assert np.max(np.abs(a - b)) <= 1e-8 * max(1.0, np.max(np.abs(b))), k
     assert ok.sum() > 0
+
+
+@pytest.mark.parametrize("units", [1, 3, 1000])
+def test_static_units_identical(units):
+    from dcu_b200.api import Context
+
+    A = W.convdiff3d(12, 20.0)
+    with Context(0) as c0, Context(0, units=units) as c1:
+        m0, r0, _ = c0.build_h(A)
+        m1, r1, _ = c1.build_h(A)
+        assert c1.units == units
+    assert np.array_equal(m0, m1) and np.array_equal(r0, r1)
