@@ -59,7 +59,9 @@ template <typename T>
 __device__ __forceinline__ double ldv(const T* p) { return (double)__ldg(p); }
 
 // One SELL-32 row: sum_k val[q] * xf(col[q]).  A warp covers one slice, so
-// each k step reads 32 consecutive slots.
+// each k step reads 32 consecutive slots.  Slots are taken 8 at a time with
+// every value and index load issued before the dependent gathers, so a thread
+// keeps up to 16 independent loads in flight.
 template <typename MT, typename IT, typename F>
 __device__ __forceinline__ double sell_row(const long long* __restrict__ off, const MT* __restrict__ val,
                                            const IT* __restrict__ ix, int r, F xf) {
@@ -68,19 +70,23 @@ __device__ __forceinline__ double sell_row(const long long* __restrict__ off, co
   const long long base = o0 + (r & 31);
   const int w = (int)((o1 - o0) >> 5);
   double acc = 0.0;
-  int k = 0;
-  for (; k + 4 <= w; k += 4) {
-    const long long q = base + 32ll * k;
-    const double a0 = ldm(val + q), a1 = ldm(val + q + 32), a2 = ldm(val + q + 64), a3 = ldm(val + q + 96);
-    const int c0 = ldcol(ix, q, r), c1 = ldcol(ix, q + 32, r), c2 = ldcol(ix, q + 64, r), c3 = ldcol(ix, q + 96, r);
-    acc += a0 * xf(c0);
-    acc += a1 * xf(c1);
-    acc += a2 * xf(c2);
-    acc += a3 * xf(c3);
-  }
-  for (; k < w; ++k) {
-    const long long q = base + 32ll * k;
-    acc += ldm(val + q) * xf(ldcol(ix, q, r));
+  for (int k0 = 0; k0 < w; k0 += 8) {
+    double av[8];
+    int cv[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      if (k0 + t < w) {
+        const long long q = base + 32ll * (k0 + t);
+        av[t] = ldm(val + q);
+        cv[t] = ldcol(ix, q, r);
+      } else {
+        av[t] = 0.0;
+        cv[t] = r;
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < 8; ++t)
+      if (k0 + t < w) acc += av[t] * xf(cv[t]);
   }
   return acc;
 }

@@ -50,6 +50,8 @@ int resolve_range(Ctx* c, int n, const dcu_options* in, dcu_options* out) {
   if (out->tol_mode != DCU_TOL_ABS && out->tol_mode != DCU_TOL_REL)
     return dcu::fail(c, DCU_ERR_ARG, "unknown tolerance mode %d", out->tol_mode);
   if (!(out->tol >= 0.0)) return dcu::fail(c, DCU_ERR_ARG, "tol must be >= 0");
+  if (out->ls_method < DCU_LS_AUTO || out->ls_method > DCU_LS_NORMAL_EQ)
+    return dcu::fail(c, DCU_ERR_ARG, "unknown least-squares method %d", out->ls_method);
   return DCU_OK;
 }
 
@@ -121,6 +123,7 @@ void dcu_options_default(dcu_options* o) {
   o->verify = 1;
   o->col_start = 0;
   o->col_end = 0;
+  o->ls_method = DCU_LS_AUTO;
 }
 
 int dcu_spai_create(dcu_spai_ctx** out, int device, int units) {
@@ -158,6 +161,7 @@ int dcu_spai_create(dcu_spai_ctx** out, int device, int units) {
   // the static schedule splits columns over `units` ranges; by default one
   // per resident warp of the column kernel
   c->units = units > 0 ? units : dcu::spai_default_units(c);
+  c->units_user = units > 0;
   *out = c;
   return DCU_OK;
 }

@@ -48,6 +48,7 @@ enum BufId {
   B_SCAL,          // solver scalars
   B_UPLOAD,        // host-API uploads
   B_SORTTMP,       // global scratch of the long-row sort
+  B_FBLIST,        // columns handed from the thread kernel to the group kernel
   B_COUNT
 };
 
@@ -62,6 +63,7 @@ struct Ctx {
   int device = 0;
   int sms = 0;
   int units = 0;
+  bool units_user = false;  // units given by the caller (else the kernels' own worker counts)
   int max_threads_sm = 2048;
   size_t smem_optin = 0;
   cudaStream_t stream = nullptr;       // the context's own non-blocking stream

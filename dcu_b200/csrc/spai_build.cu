@@ -45,6 +45,9 @@ enum {
   ST_BIG_HEAD = 7,    // queue head of the CTA kernel
   ST_DYN_HEAD = 8,    // queue head of the dynamic schedule
   ST_BIG_DONE = 9,    // columns finished by the CTA kernel
+  ST_FB_COUNT = 10,   // columns the thread kernel hands to the group kernel
+  ST_FB_HEAD = 11,    // queue head of that hand-off list
+  ST_NE_COLS = 12,    // columns finished by the thread kernel
   ST_INTS = 16,
   ST_AREA64 = 7       // long long index (ints 14-15): max candidates * (|J|+1) over queued columns
 };
@@ -76,6 +79,7 @@ struct SmallArgs {
   int* ilist;
   int* big_list;
   int* stats;
+  const int* list;    // when set: process these columns (count in stats[ST_FB_COUNT])
 };
 
 // Shared state of the two groups of a warp.  Row strides are padded so the
@@ -390,7 +394,17 @@ __global__ void __launch_bounds__(SG_BLOCK) k_spai_small(SmallArgs a) {
     }
   };
 
-  if (a.schedule == DCU_SCHED_BALANCED_COLUMNS) {
+  if (a.list) {
+    // columns handed over by the thread kernel, pulled one at a time
+    const int count = a.stats[ST_FB_COUNT];
+    for (;;) {
+      int q = 0;
+      if (lane == 0) q = atomicAdd(&a.stats[ST_FB_HEAD], 1);
+      q = __shfl_sync(gmask, q, 0, GL);
+      if (q >= count) break;
+      process(a.list[q]);
+    }
+  } else if (a.schedule == DCU_SCHED_BALANCED_COLUMNS) {
     // balanced_columns over `units` contiguous ranges; group q takes units
     // q, q + ngroups, ...
     const int total = a.col_end - a.col_start;
@@ -415,6 +429,227 @@ __global__ void __launch_bounds__(SG_BLOCK) k_spai_small(SmallArgs a) {
     atomicMax(&a.stats[ST_MAXNI], my_max_ni);
     atomicMax(&a.stats[ST_MAXNJ], my_max_nj);
     atomicAdd(&a.stats[ST_SMALL_COLS], my_cols);
+  }
+}
+
+
+// ---------------------------------------------------------------------------
+// Thread per column: the batched least-squares path of the mixed forms.
+// One thread solves min || A(:,J) m - e_k || for |J_k| <= 8 through the
+// normal equations G m = g with G = A(:,J)^T A(:,J) (sparse dot products of
+// A's columns) and g = A(k,J)^T, factored G = U^T U by Cholesky in
+// registers.  Hundreds of columns per SM are in flight, against tens on the
+// group path.  A column whose Cholesky pivots drop below tau * G_jj (the
+// normal equations' rounding would exceed the preconditioner's own precision)
+// or that exceeds the size limits is handed to the Householder group kernel.
+// ---------------------------------------------------------------------------
+constexpr int NE_BLOCK = 128;
+constexpr int NE_NJ = 8;      // max |J_k| on the thread path
+constexpr int NE_CMAX = 52;   // max entries over the J_k columns (a 3D 7-point column has 49)
+
+struct NeArgs {
+  int n;
+  const int* ptr;
+  const int* idx;
+  const double* val;
+  int col_start, col_end;
+  int schedule;
+  int units;
+  const int* chunks;
+  int nchunks;
+  double* mval;
+  double* colres;
+  int* fb_list;
+  int* stats;
+  double tau;
+};
+
+__host__ __device__ constexpr int tri(int a, int b) { return a * NE_NJ - (a * (a - 1)) / 2 + (b - a); }
+
+template <typename T>
+__global__ void __launch_bounds__(NE_BLOCK) k_spai_ne(NeArgs a) {
+  extern __shared__ __align__(16) unsigned char ne_raw[];
+  int* srow = reinterpret_cast<int*>(ne_raw);                                  // [NE_CMAX][NE_BLOCK]
+  T* sval = reinterpret_cast<T*>(ne_raw + sizeof(int) * NE_CMAX * NE_BLOCK);   // [NE_CMAX][NE_BLOCK]
+  __shared__ int s_chunk;
+  const int tid = threadIdx.x;
+  int my_cols = 0, my_max_nj = 0;
+
+  auto process = [&](int k) {
+    const int cs = __ldg(a.ptr + k);
+    const int nj = __ldg(a.ptr + k + 1) - cs;
+    my_max_nj = max(my_max_nj, nj);
+    if (nj == 0) {
+      if (a.colres) a.colres[k - a.col_start] = 1.0;
+      ++my_cols;
+      return;
+    }
+    if (nj > NE_NJ) {
+      a.fb_list[atomicAdd(&a.stats[ST_FB_COUNT], 1)] = k;
+      return;
+    }
+    int base[NE_NJ], len[NE_NJ], cb[NE_NJ];
+    int cand = 0;
+#pragma unroll
+    for (int j = 0; j < NE_NJ; ++j) {
+      base[j] = 0;
+      len[j] = 0;
+      if (j < nj) {
+        const int col = __ldg(a.idx + cs + j);
+        base[j] = __ldg(a.ptr + col);
+        len[j] = __ldg(a.ptr + col + 1) - base[j];
+      }
+      cb[j] = cand;
+      cand += len[j];
+    }
+    if (cand > NE_CMAX) {
+      a.fb_list[atomicAdd(&a.stats[ST_FB_COUNT], 1)] = k;
+      return;
+    }
+    bool sorted = true;
+#pragma unroll
+    for (int j = 0; j < NE_NJ; ++j) {
+      int prev = -1;
+      for (int q = 0; q < len[j]; ++q) {
+        const int r = __ldg(a.idx + base[j] + q);
+        sorted = sorted && (r > prev);
+        prev = r;
+        srow[(cb[j] + q) * NE_BLOCK + tid] = r;
+        sval[(cb[j] + q) * NE_BLOCK + tid] = (T)__ldg(a.val + base[j] + q);
+      }
+    }
+    // G (upper triangle) and g = A(k, J)^T
+    T G[NE_NJ * (NE_NJ + 1) / 2], g[NE_NJ];
+#pragma unroll
+    for (int i = 0; i < NE_NJ * (NE_NJ + 1) / 2; ++i) G[i] = T(0);
+#pragma unroll
+    for (int j = 0; j < NE_NJ; ++j) g[j] = T(0);
+#pragma unroll
+    for (int ja = 0; ja < NE_NJ; ++ja) {
+      for (int p = cb[ja]; p < cb[ja] + len[ja]; ++p) {
+        const int r = srow[p * NE_BLOCK + tid];
+        const T v = sval[p * NE_BLOCK + tid];
+        if (r == k) g[ja] += v;
+        G[tri(ja, ja)] += v * v;
+      }
+    }
+    if (sorted) {
+      // rows ascending in every column: merge each pair of columns
+#pragma unroll
+      for (int ja = 0; ja < NE_NJ; ++ja) {
+#pragma unroll
+        for (int jb = ja + 1; jb < NE_NJ; ++jb) {
+          int i = cb[ja], j = cb[jb];
+          const int ie = i + len[ja], je = j + len[jb];
+          T acc = T(0);
+          while (i < ie && j < je) {
+            const int ra = srow[i * NE_BLOCK + tid], rb = srow[j * NE_BLOCK + tid];
+            if (ra == rb) acc += sval[i * NE_BLOCK + tid] * sval[j * NE_BLOCK + tid];
+            i += (ra <= rb) ? 1 : 0;
+            j += (rb <= ra) ? 1 : 0;
+          }
+          G[tri(ja, jb)] += acc;
+        }
+      }
+    } else {
+#pragma unroll
+      for (int ja = 0; ja < NE_NJ; ++ja) {
+        for (int p = cb[ja]; p < cb[ja] + len[ja]; ++p) {
+          const int r = srow[p * NE_BLOCK + tid];
+          const T v = sval[p * NE_BLOCK + tid];
+#pragma unroll
+          for (int jb = ja + 1; jb < NE_NJ; ++jb) {
+            T acc = T(0);
+            for (int q = cb[jb]; q < cb[jb] + len[jb]; ++q)
+              if (srow[q * NE_BLOCK + tid] == r) acc += sval[q * NE_BLOCK + tid];
+            G[tri(ja, jb)] += v * acc;
+          }
+        }
+      }
+    }
+    // pad to 8 x 8 with the identity, factor G = U^T U in place
+#pragma unroll
+    for (int j = 0; j < NE_NJ; ++j)
+      if (j >= nj) G[tri(j, j)] = T(1);
+    bool ok = true;
+#pragma unroll
+    for (int j = 0; j < NE_NJ; ++j) {
+      const T gjj = G[tri(j, j)];
+      T d = gjj;
+#pragma unroll
+      for (int p = 0; p < j; ++p) d -= G[tri(p, j)] * G[tri(p, j)];
+      if (!(d > (T)a.tau * gjj) || !isfinite((double)d)) ok = false;
+      const T ujj = sqrt(d > T(0) ? d : T(1));
+      const T inv = T(1) / ujj;
+      G[tri(j, j)] = ujj;
+#pragma unroll
+      for (int i = j + 1; i < NE_NJ; ++i) {
+        T t = G[tri(j, i)];
+#pragma unroll
+        for (int p = 0; p < j; ++p) t -= G[tri(p, j)] * G[tri(p, i)];
+        G[tri(j, i)] = t * inv;
+      }
+    }
+    if (!ok) {
+      a.fb_list[atomicAdd(&a.stats[ST_FB_COUNT], 1)] = k;
+      return;
+    }
+    // U^T y = g, U x = y
+    T y[NE_NJ];
+#pragma unroll
+    for (int j = 0; j < NE_NJ; ++j) {
+      T t = g[j];
+#pragma unroll
+      for (int p = 0; p < j; ++p) t -= G[tri(p, j)] * y[p];
+      y[j] = t / G[tri(j, j)];
+    }
+#pragma unroll
+    for (int j = NE_NJ - 1; j >= 0; --j) {
+      T t = y[j];
+#pragma unroll
+      for (int p = j + 1; p < NE_NJ; ++p) t -= G[tri(j, p)] * y[p];
+      y[j] = t / G[tri(j, j)];
+    }
+    double gx = 0.0;
+#pragma unroll
+    for (int j = 0; j < NE_NJ; ++j)
+      if (j < nj) {
+        a.mval[cs + j] = (double)y[j];
+        gx += (double)g[j] * (double)y[j];
+      }
+    // || A(:,J) m - e_k ||^2 = 1 - g^T m at the least-squares solution
+    if (a.colres) a.colres[k - a.col_start] = sqrt(fmax(0.0, 1.0 - gx));
+    ++my_cols;
+  };
+
+  if (a.schedule == DCU_SCHED_BALANCED_COLUMNS) {
+    // balanced_columns over `units` ranges; a block takes units b, b + grid, ...
+    // and its threads walk the range together
+    const int total = a.col_end - a.col_start;
+    const int basec = total / a.units, rem = total % a.units;
+    for (int u = blockIdx.x; u < a.units; u += gridDim.x) {
+      const int start = a.col_start + u * basec + min(u, rem);
+      const int end = start + basec + (u < rem ? 1 : 0);
+      for (int k = start + tid; k < end; k += NE_BLOCK) process(k);
+    }
+  } else {
+    for (;;) {
+      if (tid == 0) s_chunk = atomicAdd(&a.stats[ST_DYN_HEAD], 1);
+      __syncthreads();
+      const int ch = s_chunk;
+      __syncthreads();
+      if (ch >= a.nchunks) break;
+      for (int k = a.chunks[ch] + tid; k < a.chunks[ch + 1]; k += NE_BLOCK) process(k);
+    }
+  }
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) {
+    my_cols += __shfl_xor_sync(0xffffffffu, my_cols, d);
+    my_max_nj = max(my_max_nj, __shfl_xor_sync(0xffffffffu, my_max_nj, d));
+  }
+  if ((tid & 31) == 0) {
+    atomicAdd(&a.stats[ST_NE_COLS], my_cols);
+    atomicMax(&a.stats[ST_MAXNJ], my_max_nj);
   }
 }
 
@@ -770,6 +1005,32 @@ int run_large(Ctx* c, LargeArgs& a, int nbig) {
   return DCU_OK;
 }
 
+template <typename T>
+int run_ne(Ctx* c, NeArgs a) {
+  const size_t smem = (sizeof(int) + sizeof(T)) * NE_CMAX * NE_BLOCK;
+  DCU_CUDA(c, cudaFuncSetAttribute(k_spai_ne<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spai_ne<T>, NE_BLOCK, smem) != cudaSuccess ||
+      per_sm < 1) {
+    cudaGetLastError();
+    per_sm = 1;
+  }
+  const int grid = c->sms * per_sm;
+  if (a.units <= 0) a.units = grid;
+  if (a.schedule == DCU_SCHED_BALANCED_NNZ) {
+    const int nchunks = grid * 8;
+    DCU_TRY(ensure(c, B_CHUNKS, sizeof(int) * (size_t)(nchunks + 1)));
+    int* bounds = bp<int>(c, B_CHUNKS);
+    k_nnz_chunks<<<(nchunks + 256) / 256, 256, 0, c->stream>>>(a.ptr, a.col_start, a.col_end, nchunks, bounds);
+    DCU_LAUNCHED(c, "k_nnz_chunks");
+    a.chunks = bounds;
+    a.nchunks = nchunks;
+  }
+  k_spai_ne<T><<<grid, NE_BLOCK, smem, c->stream>>>(a);
+  DCU_LAUNCHED(c, "k_spai_ne");
+  return DCU_OK;
+}
+
 struct Prepared {
   SmallArgs sa;
   int grid = 0;
@@ -810,13 +1071,38 @@ int read_stats(Ctx* c, int* host) {
 
 template <typename T>
 int build_typed(Ctx* c, int n, const int* ptr, const int* idx, const double* val, int col_start, int col_end,
-                int schedule, double* mval, double* colres, dcu_build_info* info) {
+                int schedule, bool thread_path, double* mval, double* colres, dcu_build_info* info) {
   Prepared P;
   DCU_TRY(prepare(c, n, ptr, idx, val, col_start, col_end, schedule, &P));
   P.sa.mval = mval;
   P.sa.colres = colres;
-  DCU_TRY((run_small<T, MODE_BUILD>(c, P.sa, P.grid)));
   int st[ST_INTS];
+  if (thread_path) {
+    // thread per column first; its hand-offs go to the group kernel
+    DCU_TRY(ensure(c, B_FBLIST, sizeof(int) * (size_t)(col_end - col_start)));
+    NeArgs na{};
+    na.n = n;
+    na.ptr = ptr;
+    na.idx = idx;
+    na.val = val;
+    na.col_start = col_start;
+    na.col_end = col_end;
+    na.schedule = schedule;
+    na.units = c->units_user ? c->units : 0;
+    na.mval = mval;
+    na.colres = colres;
+    na.fb_list = bp<int>(c, B_FBLIST);
+    na.stats = P.stats;
+    na.tau = sizeof(T) == sizeof(float) ? 1e-3 : 1e-8;
+    DCU_TRY(run_ne<T>(c, na));
+    DCU_TRY(read_stats(c, st));
+    if (st[ST_FB_COUNT] > 0) {
+      P.sa.list = na.fb_list;
+      DCU_TRY((run_small<T, MODE_BUILD>(c, P.sa, P.grid)));
+    }
+  } else {
+    DCU_TRY((run_small<T, MODE_BUILD>(c, P.sa, P.grid)));
+  }
   DCU_TRY(read_stats(c, st));
   const int nbig = st[ST_BIG_COUNT];
   if (nbig > 0) {
@@ -841,7 +1127,7 @@ int build_typed(Ctx* c, int n, const int* ptr, const int* idx, const double* val
   }
   if (info) {
     info->cols_total = col_end - col_start;
-    info->cols_small = st[ST_SMALL_COLS];
+    info->cols_small = st[ST_SMALL_COLS] + st[ST_NE_COLS];
     info->cols_large = st[ST_BIG_DONE];
     info->cols_singular = st[ST_SINGULAR];
     info->max_nj = st[ST_MAXNJ] > st[ST_BIG_MAXNJ] ? st[ST_MAXNJ] : st[ST_BIG_MAXNJ];
@@ -870,9 +1156,14 @@ int spai_build(Ctx* c, int n, int nnz, const int* ptr, const int* idx, const dou
   if (col_start != 0 || col_end != n)
     DCU_CUDA(c, cudaMemsetAsync(mval, 0, sizeof(double) * (size_t)(nnz > 0 ? nnz : 1), c->stream));
   if (col_end <= col_start) return DCU_OK;
+  // FP64 (the plain form): Householder on every column unless the normal
+  // equations are asked for.  Mixed forms: the thread-per-column path first,
+  // Householder for the columns it hands over, unless Householder is asked for.
   if (opt->precision == DCU_PREC_FP64)
-    return build_typed<double>(c, n, ptr, idx, val, col_start, col_end, opt->schedule, mval, colres, info);
-  return build_typed<float>(c, n, ptr, idx, val, col_start, col_end, opt->schedule, mval, colres, info);
+    return build_typed<double>(c, n, ptr, idx, val, col_start, col_end, opt->schedule,
+                               opt->ls_method == DCU_LS_NORMAL_EQ, mval, colres, info);
+  return build_typed<float>(c, n, ptr, idx, val, col_start, col_end, opt->schedule, opt->ls_method != DCU_LS_HOUSEHOLDER,
+                            mval, colres, info);
 }
 
 int spai_pattern(Ctx* c, int n, const int* ptr, const int* idx, int col_start, int col_end, int* icount,

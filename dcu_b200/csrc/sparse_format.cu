@@ -34,17 +34,54 @@ __global__ void k_row_scatter(const int* __restrict__ ptr, const int* __restrict
   }
 }
 
-constexpr int kThreadSortMax = 64;
+constexpr int kRegSortMax = 16;     // rows sorted in registers by one thread
+constexpr int kThreadSortMax = 64;  // rows sorted in place by one thread
 
-// Rows up to kThreadSortMax entries: insertion sort by one thread; longer rows
+// Rows up to kRegSortMax entries: loaded into registers as (col << 32 | slot)
+// keys, sorted with a static insertion network, written back only when out
+// of order.  Rows up to kThreadSortMax: insertion sort in place.  Longer rows
 // are queued for the block sort.  Column indices inside a row are distinct
 // (a CSC column lists each row once), so the order is unique.
 __global__ void k_row_sort_short(const int* __restrict__ rptr, int n, int* __restrict__ rcol,
                                  int* __restrict__ rperm, int* __restrict__ long_rows,
                                  int* __restrict__ long_count) {
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
-    int s = rptr[r], e = rptr[r + 1];
-    int len = e - s;
+    const int s = rptr[r], e = rptr[r + 1];
+    const int len = e - s;
+    if (len <= kRegSortMax) {
+      unsigned long long key[kRegSortMax];
+      bool sorted = true;
+      int prev = -1;
+#pragma unroll
+      for (int i = 0; i < kRegSortMax; ++i) {
+        if (i < len) {
+          const int cc = rcol[s + i];
+          sorted = sorted && (cc > prev);
+          prev = cc;
+          key[i] = ((unsigned long long)(unsigned)cc << 32) | (unsigned)rperm[s + i];
+        } else {
+          key[i] = ~0ull;
+        }
+      }
+      if (sorted) continue;
+#pragma unroll
+      for (int i = 1; i < kRegSortMax; ++i) {
+#pragma unroll
+        for (int q = i; q > 0; --q) {
+          const unsigned long long lo = min(key[q - 1], key[q]), hi = max(key[q - 1], key[q]);
+          key[q - 1] = lo;
+          key[q] = hi;
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < kRegSortMax; ++i) {
+        if (i < len) {
+          rcol[s + i] = (int)(key[i] >> 32);
+          rperm[s + i] = (int)(key[i] & 0xffffffffu);
+        }
+      }
+      continue;
+    }
     if (len > kThreadSortMax) {
       long_rows[atomicAdd(long_count, 1)] = r;
       atomicMax(long_count + 1, len);

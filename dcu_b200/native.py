@@ -18,6 +18,8 @@ OK, ERR_ARG, ERR_CUDA, ERR_ALLOC, ERR_NO_DEVICE, ERR_LIMIT = range(6)
 SCHED_BALANCED_COLUMNS, SCHED_BALANCED_NNZ = 0, 1
 # dcu_precision
 PREC_FP64, PREC_MIXED_FP32, PREC_MIXED_BF16, PREC_M_FP32, PREC_M_BF16 = 0, 1, 2, 3, 4
+# dcu_ls_method
+LS_AUTO, LS_HOUSEHOLDER, LS_NORMAL_EQ = 0, 1, 2
 # dcu_tol_mode
 TOL_ABS, TOL_REL = 0, 1
 # dcu_solve_status
@@ -26,7 +28,8 @@ SOLVE_CONVERGED, SOLVE_MAXITER, SOLVE_BREAKDOWN = 0, 1, 2
 
 class Options(C.Structure):
     _fields_ = [("schedule", C.c_int), ("precision", C.c_int), ("tol_mode", C.c_int), ("maxiter", C.c_int),
-                ("tol", C.c_double), ("verify", C.c_int), ("col_start", C.c_int), ("col_end", C.c_int)]
+                ("tol", C.c_double), ("verify", C.c_int), ("col_start", C.c_int), ("col_end", C.c_int),
+                ("ls_method", C.c_int)]
 
 
 class BuildInfo(C.Structure):

@@ -67,6 +67,17 @@ typedef enum {
   DCU_PREC_M_BF16 = 4     /* as M_FP32 with M stored as BF16                               */
 } dcu_precision;
 
+/* Least-squares method of the SPAI build. */
+typedef enum {
+  DCU_LS_AUTO = 0,        /* FP64 form: Householder; mixed forms: NORMAL_EQ        */
+  DCU_LS_HOUSEHOLDER = 1, /* Householder QR for every column                       */
+  DCU_LS_NORMAL_EQ = 2    /* columns with |J| <= 8 and <= 52 entries over J: one
+                             thread per column, normal equations + Cholesky in the
+                             form's precision; a column whose Cholesky pivot falls
+                             below tau G_jj (tau 1e-3 FP32, 1e-8 FP64) or that
+                             exceeds those sizes goes to Householder QR            */
+} dcu_ls_method;
+
 /* Stopping rule. */
 typedef enum {
   DCU_TOL_ABS = 0,        /* ||r||_2 < tol (the reference, bicgstab_solver.h:229) */
@@ -111,6 +122,7 @@ typedef struct {
                              the threshold (residual replacement); 0: stop on
                              the recurrence residual exactly as the reference */
   int col_start, col_end; /* SPAI column range; col_end <= 0 means n          */
+  int ls_method;          /* dcu_ls_method                                  */
 } dcu_options;
 
 /* Fill *opt with the defaults of the BASELINE configs: balanced_columns,

@@ -85,3 +85,30 @@ def test_static_units_identical(units):
         m1, r1, _ = c1.build_h(A)
         assert c1.units == units
     assert np.array_equal(m0, m1) and np.array_equal(r0, r1)
+
+
+@pytest.mark.parametrize("ls", [N.LS_AUTO, N.LS_HOUSEHOLDER])
+@pytest.mark.parametrize("name,A", [("cd3d_16", W.convdiff3d(16, 20.0)), ("circuit", W.circuit_like()),
+                                    ("cd2d_64", W.convdiff2d(64, 10.0))])
+def test_spai_fp32_methods(ctx, ls, name, A):
+    """FP32 least squares: thread-per-column normal equations (with hand-off
+    to Householder) and Householder alone both match the FP64 oracle."""
+    m_h, res_h, _, _ = oracle.spai(A, "householder")
+    m, res, info = ctx.build_h(A, precision=N.PREC_MIXED_BF16, ls_method=ls)
+    assert info.cols_small + info.cols_large == A.n
+    assert info.cols_singular == 0
+    for k in range(A.n):   # per column, relative to the column's own scale
+        a, b = m[A.ptr[k]:A.ptr[k + 1]], m_h[A.ptr[k]:A.ptr[k + 1]]
+        if len(b):
+            assert np.max(np.abs(a - b)) <= RTOL_FP32 * 10 * np.max(np.abs(b)), (k, a, b)
+    assert np.max(np.abs(res - res_h)) < 1e-3
+
+
+@pytest.mark.parametrize("name,A", [("cd3d_16", W.convdiff3d(16, 20.0)), ("circuit", W.circuit_like()),
+                                    ("cd2d_64", W.convdiff2d(64, 10.0))])
+def test_spai_fp64_normal_equations(ctx, name, A):
+    """FP64 normal equations (hand-off below pivot ratio 1e-8) against the FP64 oracle."""
+    m_h, res_h, _, _ = oracle.spai(A, "householder")
+    m, res, info = ctx.build_h(A, precision=N.PREC_FP64, ls_method=N.LS_NORMAL_EQ)
+    assert info.cols_small + info.cols_large == A.n
+    assert rel_err(m, m_h) < 1e-9
