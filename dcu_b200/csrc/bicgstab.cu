@@ -162,7 +162,12 @@ struct BiArgs {
   Scal* S;
 };
 
-__device__ __forceinline__ bool finished(const Scal* S) { return *(volatile const int*)&S->done != 0; }
+// Kernels K1..K5 are launched with programmatic dependent launch: their blocks
+// may start while the previous kernel drains, and wait here for its results.
+__device__ __forceinline__ bool finished(const Scal* S) {
+  cudaGridDependencySynchronize();
+  return *(volatile const int*)&S->done != 0;
+}
 
 __device__ __forceinline__ bool bad(double v) { return !isfinite(v); }
 
@@ -381,6 +386,21 @@ __global__ void __launch_bounds__(BI_BLOCK) k_bi_true(BiArgs<MT, IT, VT> a, int 
   }
 }
 
+template <typename K, typename A>
+cudaError_t launch_pdl(K kernel, int grid, cudaStream_t st, const A& args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(BI_BLOCK);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, args);
+}
+
 template <typename MT, typename IT, typename VT>
 int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval, const IT* ix, const double* b,
                double* x, const dcu_options* opt, dcu_solve_info* info) {
@@ -445,14 +465,19 @@ int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval,
   if (!ge) {
     cudaGraph_t g = nullptr;
     DCU_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    for (int i = 0; i < CHUNK_ITERS; ++i) {
-      k_bi_py<MT, IT, VT><<<g_py, BI_BLOCK, 0, c->stream>>>(a);
-      k_bi_ay<MT, IT, VT><<<g_ay, BI_BLOCK, 0, c->stream>>>(a);
-      k_bi_sz<MT, IT, VT><<<g_sz, BI_BLOCK, 0, c->stream>>>(a);
-      k_bi_az<MT, IT, VT><<<g_az, BI_BLOCK, 0, c->stream>>>(a);
-      k_bi_xr<MT, IT, VT><<<g_xr, BI_BLOCK, 0, c->stream>>>(a);
+    cudaError_t le = cudaSuccess;
+    for (int i = 0; i < CHUNK_ITERS && le == cudaSuccess; ++i) {
+      le = launch_pdl(k_bi_py<MT, IT, VT>, g_py, c->stream, a);
+      if (le == cudaSuccess) le = launch_pdl(k_bi_ay<MT, IT, VT>, g_ay, c->stream, a);
+      if (le == cudaSuccess) le = launch_pdl(k_bi_sz<MT, IT, VT>, g_sz, c->stream, a);
+      if (le == cudaSuccess) le = launch_pdl(k_bi_az<MT, IT, VT>, g_az, c->stream, a);
+      if (le == cudaSuccess) le = launch_pdl(k_bi_xr<MT, IT, VT>, g_xr, c->stream, a);
     }
     cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (le != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      return cuda_fail(c, le, "cudaLaunchKernelEx (capture)", __FILE__, __LINE__);
+    }
     if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture", __FILE__, __LINE__);
     GraphSlot ne;
     ne.key = key;
