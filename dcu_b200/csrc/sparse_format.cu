@@ -10,6 +10,8 @@
 //          reads 32 consecutive slots per k (128-byte lines for FP32/int32,
 //          256 bytes for FP64).  Padding slots carry column = r and perm = -1.
 //          del int16 holds col - r when every |col - r| < 32768.
+#include <mutex>
+
 #include "internal.cuh"
 
 namespace dcu {
@@ -388,4 +390,169 @@ int csr_values(Ctx* c, int nnz, const int* rperm, const double* val, double* rva
   return DCU_OK;
 }
 
+// ---------------------------------------------------------------------------
+// CSC -> CSR without any device allocation (dcu_csc_to_csr_noalloc_d).
+//
+// For callers that must not allocate device memory: code that runs inside a
+// framework whose memory pool owns the device (an out-of-band cudaMalloc
+// fragments or exceeds its budget), or a latency-critical path that cannot
+// afford cudaMalloc/cudaFree and the device synchronisation cudaFree implies.
+// The scratch of the conversion lives in one file-scope __device__ array of
+// fixed size (every GPU that loads this library holds it until the process
+// exits).  Limits: n <= kNoAllocMaxN, nnz <= kNoAllocMaxNnz, no row longer
+// than kSmemSortMax entries.  Every call shares the array and finds the last
+// call's contents, so the parts that must start at zero are cleared on each
+// call; calls that overlap on the GPU (other streams, other host threads on
+// the same device) race on it.
+// ---------------------------------------------------------------------------
+constexpr int kNoAllocMaxN = 131072;
+constexpr int kNoAllocMaxNnz = 1048576;
+constexpr size_t kNoAllocCnt = 0;                                             // int[n + 1]
+constexpr size_t kNoAllocLong = kNoAllocCnt + sizeof(int) * (kNoAllocMaxN + 64);  // int[n + 2]
+constexpr size_t kNoAllocPerm = kNoAllocLong + sizeof(int) * (kNoAllocMaxN + 64); // int[nnz]
+constexpr size_t kNoAllocFlags = kNoAllocPerm + sizeof(int) * kNoAllocMaxNnz;    // int[8]
+constexpr size_t kNoAllocBytes = kNoAllocFlags + 256;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+namespace {
+
+// Exclusive scan of n <= kNoAllocMaxN counts by one block of 1024 threads
+// (each thread scans a contiguous chunk, then the chunk totals are scanned).
+constexpr int kSmallScanThreads = 1024;
+__global__ void __launch_bounds__(kSmallScanThreads) k_scan_small(const int* __restrict__ in, int* __restrict__ out,
+                                                                   int n) {
+  __shared__ int tot[kSmallScanThreads];
+  const int per = (n + kSmallScanThreads - 1) / kSmallScanThreads;
+  const int b = threadIdx.x * per, e = min(n, b + per);
+  int run = 0;
+  for (int i = b; i < e; ++i) run += in[i];
+  tot[threadIdx.x] = run;
+  __syncthreads();
+  for (int d = 1; d < kSmallScanThreads; d <<= 1) {
+    const int v = (threadIdx.x >= d) ? tot[threadIdx.x - d] : 0;
+    __syncthreads();
+    tot[threadIdx.x] += v;
+    __syncthreads();
+  }
+  int acc = tot[threadIdx.x] - run;
+  for (int i = b; i < e; ++i) {
+    out[i] = acc;
+    acc += in[i];
+  }
+  if (threadIdx.x == kSmallScanThreads - 1) out[n] = tot[kSmallScanThreads - 1];
+}
+
+// Long rows (more than kThreadSortMax entries) by one block each, shared
+// memory only; a row above kSmemSortMax entries sets flags[1] and is skipped.
+__global__ void __launch_bounds__(512) k_row_sort_long_smem(const int* __restrict__ rptr, const int* __restrict__ rows,
+                                                            const int* __restrict__ count, int* __restrict__ rcol,
+                                                            int* __restrict__ rperm, int* __restrict__ flags) {
+  extern __shared__ unsigned long long skey2[];
+  const int nrows = *count;
+  for (int q = blockIdx.x; q < nrows; q += gridDim.x) {
+    const int r = rows[q];
+    const int s0 = rptr[r], len = rptr[r + 1] - s0;
+    if (len > kSmemSortMax) {
+      if (threadIdx.x == 0) atomicOr(&flags[1], 1);
+      continue;
+    }
+    int np2 = 1;
+    while (np2 < len) np2 <<= 1;
+    for (int i = threadIdx.x; i < np2; i += blockDim.x)
+      skey2[i] = (i < len) ? ((unsigned long long)(unsigned)rcol[s0 + i] << 32 | (unsigned)rperm[s0 + i]) : ~0ull;
+    __syncthreads();
+    bitonic_block(skey2, np2);
+    for (int i = threadIdx.x; i < len; i += blockDim.x) {
+      rcol[s0 + i] = (int)(skey2[i] >> 32);
+      rperm[s0 + i] = (int)(skey2[i] & 0xffffffffu);
+    }
+    __syncthreads();
+  }
+}
+
+// Device address of g_noalloc_scratch, looked up once per device (with that
+// device current) on the first call there.
+void* noalloc_scratch_for_device(int device, cudaError_t* err) {
+  static std::mutex mu;
+  static void* addr[64] = {nullptr};
+  *err = cudaSuccess;
+  if (device < 0 || device >= 64) {
+    *err = cudaErrorInvalidDevice;
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[device]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) {
+      *err = e;
+      return nullptr;
+    }
+    addr[device] = p;
+  }
+  return addr[device];
+}
+
+}  // namespace
 }  // namespace dcu
+
+extern "C" int dcu_csc_to_csr_noalloc_d(int n, int nnz, const int* ptr, const int* idx, const double* val, int* rptr,
+                                        int* ridx, double* rval, void* stream_ptr) {
+  using namespace dcu;
+  if (n <= 0 || nnz < 0 || !ptr || !rptr || (nnz > 0 && (!idx || !ridx))) return DCU_ERR_ARG;
+  if (n > kNoAllocMaxN || nnz > kNoAllocMaxNnz) return DCU_ERR_LIMIT;
+  cudaStream_t st = (cudaStream_t)stream_ptr;
+  int device = 0;
+  if (cudaGetDevice(&device) != cudaSuccess) return DCU_ERR_CUDA;
+  cudaError_t e = cudaSuccess;
+  char* base = static_cast<char*>(noalloc_scratch_for_device(device, &e));
+  if (!base) return e == cudaErrorInvalidDevice ? DCU_ERR_NO_DEVICE : DCU_ERR_CUDA;
+  int* cnt = reinterpret_cast<int*>(base + kNoAllocCnt);
+  int* longrows = reinterpret_cast<int*>(base + kNoAllocLong);
+  int* longcount = longrows + n;  // [0] count, [1] longest
+  int* perm = reinterpret_cast<int*>(base + kNoAllocPerm);
+  int* flags = reinterpret_cast<int*>(base + kNoAllocFlags);  // [0] malformed input, [1] row too long
+  const int grid_n = (n + 255) / 256 < 1184 ? (n + 255) / 256 : 1184;
+  const int grid_z = (nnz + 255) / 256 < 1184 ? ((nnz + 255) / 256 > 0 ? (nnz + 255) / 256 : 1) : 1184;
+  int host_flags[2] = {0, 0};
+#define NOALLOC_CHECK(call)                    \
+  do {                                         \
+    if ((call) != cudaSuccess) {               \
+      cudaGetLastError();                      \
+      return DCU_ERR_CUDA;                     \
+    }                                          \
+  } while (0)
+  // what must start at zero: the row counts, the long-row counters, the flags
+  NOALLOC_CHECK(cudaMemsetAsync(cnt, 0, sizeof(int) * (size_t)(n + 1), st));
+  NOALLOC_CHECK(cudaMemsetAsync(longcount, 0, 2 * sizeof(int), st));
+  NOALLOC_CHECK(cudaMemsetAsync(flags, 0, 8 * sizeof(int), st));
+  k_validate_csc<<<grid_n > grid_z ? grid_n : grid_z, 256, 0, st>>>(ptr, idx, n, nnz, flags);
+  NOALLOC_CHECK(cudaGetLastError());
+  NOALLOC_CHECK(cudaMemcpyAsync(host_flags, flags, sizeof(int), cudaMemcpyDeviceToHost, st));
+  NOALLOC_CHECK(cudaStreamSynchronize(st));
+  if (host_flags[0]) return DCU_ERR_ARG;
+  if (nnz > 0) {
+    k_row_count<<<grid_z, 256, 0, st>>>(idx, nnz, cnt);
+    NOALLOC_CHECK(cudaGetLastError());
+  }
+  k_scan_small<<<1, kSmallScanThreads, 0, st>>>(cnt, rptr, n);
+  NOALLOC_CHECK(cudaGetLastError());
+  NOALLOC_CHECK(cudaMemsetAsync(cnt, 0, sizeof(int) * (size_t)(n + 1), st));
+  k_row_scatter<<<grid_n, 256, 0, st>>>(ptr, idx, n, rptr, cnt, ridx, perm);
+  NOALLOC_CHECK(cudaGetLastError());
+  k_row_sort_short<<<grid_n, 256, 0, st>>>(rptr, n, ridx, perm, longrows, longcount);
+  NOALLOC_CHECK(cudaGetLastError());
+  const size_t smem = sizeof(unsigned long long) * kSmemSortMax;
+  NOALLOC_CHECK(cudaFuncSetAttribute(k_row_sort_long_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_row_sort_long_smem<<<148, 512, smem, st>>>(rptr, longrows, longcount, ridx, perm, flags);
+  NOALLOC_CHECK(cudaGetLastError());
+  if (val && rval && nnz > 0) {
+    k_gather_f64<<<grid_z, 256, 0, st>>>(perm, val, nnz, rval);
+    NOALLOC_CHECK(cudaGetLastError());
+  }
+  NOALLOC_CHECK(cudaMemcpyAsync(host_flags, flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+  NOALLOC_CHECK(cudaStreamSynchronize(st));
+#undef NOALLOC_CHECK
+  return host_flags[1] ? DCU_ERR_LIMIT : DCU_OK;
+}

@@ -61,6 +61,7 @@ SIGNATURES = {
     "dcu_spai_build_d": (_i, [_vp, _i, _i, _vp, _vp, _vp, _OPT, _vp, _vp, C.POINTER(BuildInfo)]),
     "dcu_spai_build_h": (_i, [_vp, _i, _i, _vp, _vp, _vp, _OPT, _vp, _vp, C.POINTER(BuildInfo)]),
     "dcu_csc_to_csr_d": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "dcu_csc_to_csr_noalloc_d": (_i, [_i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "dcu_bicgstab_d": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _OPT, C.POINTER(SolveInfo)]),
     "dcu_bicgstab_h": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _OPT, C.POINTER(SolveInfo)]),
     "dcu_spai_solve_d": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _OPT, _vp, C.POINTER(BuildInfo),

@@ -181,6 +181,24 @@ int dcu_spai_build_h(dcu_spai_ctx* ctx, int n, int nnz, const int* ptr, const in
 int dcu_csc_to_csr_d(dcu_spai_ctx* ctx, int n, int nnz, const int* ptr, const int* idx,
                      const double* val, int* rptr, int* ridx, double* rval);
 
+/* CSC -> CSR exactly as dcu_csc_to_csr_d, for callers that cannot allocate
+ * device memory: code running under a framework's memory pool that owns the
+ * device (an out-of-band cudaMalloc fragments or exceeds its budget) or a
+ * latency-critical path that cannot take cudaMalloc/cudaFree and the device
+ * synchronisation cudaFree implies.  No context, no cudaMalloc/cudaFree, no
+ * allocating library call: the scratch is one fixed __device__ array of about
+ * 5 MB in this library, which every GPU that loads the library holds until the
+ * process exits.  Limits: n <= 131072, nnz <= 1048576 (DCU_ERR_LIMIT beyond),
+ * no row longer than 8192 entries (DCU_ERR_LIMIT after the call).  Runs on
+ * `stream` (a cudaStream_t, NULL = legacy default) on the current device and
+ * returns after it finished there.  The first call on a device looks up the
+ * array's device address there; make that first call before any stream
+ * capture.  Every call reuses the same array (the parts that must start at
+ * zero are cleared each time), so calls that overlap on one GPU race.
+ * No counterpart in the reference. */
+int dcu_csc_to_csr_noalloc_d(int n, int nnz, const int* ptr, const int* idx, const double* val,
+                             int* rptr, int* ridx, double* rval, void* stream);
+
 /* ---- BiCGSTAB --------------------------------------------------------------- */
 
 /* Right-preconditioned BiCGSTAB for A x = b with preconditioner M (values on
