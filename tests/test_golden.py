@@ -1,0 +1,66 @@
+"""The oracle against its committed golden fixtures (tests/golden/golden.json,
+made by tests/golden/make_golden.py), and the library's reader against the
+reference fixture digests where the fixture is present."""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from dcu_b200 import workloads as W
+
+GOLDEN = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "golden.json")))
+
+CASES = {
+    "convdiff2d_64_pe10": lambda: W.convdiff2d(64, 10.0),
+    "convdiff3d_16_pe20": lambda: W.convdiff3d(16, 20.0),
+    "circuit_like_seed2024": lambda: W.circuit_like(),
+}
+
+
+def digest(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()[:16]
+
+
+def rhs(A, kind):
+    if kind == "ones_product":
+        return W.rhs_ones_product(A)
+    if kind == "uniform":
+        return np.random.Generator(np.random.PCG64(11)).uniform(-1, 1, A.n)
+    return W.rhs_from_solution(A, seed=7)[0]
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_oracle_reproduces_golden(name):
+    g = GOLDEN[name]
+    A = CASES[name]()
+    assert (A.n, A.nnz) == (g["n"], g["nnz"])
+    cnt, _, il = oracle.pattern(A)
+    assert digest(il) == g["pattern_sha"] and digest(cnt) == g["icount_sha"]
+    m, colres, _, sing = oracle.spai(A, "mgs")
+    assert abs(m.sum() - g["m_sum"]) <= 1e-12 * max(1.0, abs(g["m_sum"]))
+    assert np.allclose(m[:8], g["m_head"], rtol=1e-13, atol=0)
+    ref = oracle.bicgstab(A, m, np.ones(A.n), np.ones(A.n), tol=1e-7, tol_mode="abs", maxiter=10000)
+    assert ref["iters"] == g["iters_reference_settings"]
+
+
+def test_survey_reference_algorithm_facts():
+    # 64x64 Pe 10: 43 iterations with the reference's solver settings, 45 with
+    # the config's (b = A 1, x0 = 0, relative 1e-8)
+    g = GOLDEN["convdiff2d_64_pe10"]
+    assert g["iters_reference_settings"] == 43
+    assert g["iters_config_settings"] == 45
+
+
+def test_reader_matches_fixture_digests():
+    path = "/root/reference/matrices/circuit_2.mtx"
+    if not os.path.exists(path):
+        pytest.skip("reference fixture absent")
+    from dcu_b200.api import mtx_read
+
+    A = mtx_read(path)
+    g = GOLDEN["circuit_2_mtx"]
+    assert (A.n, A.nnz) == (g["n"], g["nnz"])
+    assert digest(A.ptr) == g["ptr_sha"] and digest(A.idx) == g["idx_sha"] and digest(A.val) == g["val_sha"]
