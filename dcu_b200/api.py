@@ -166,6 +166,18 @@ class Context:
                                            _p(x_d), C.byref(o), C.byref(info)))
         return info
 
+    def bicgstab_transpose_d(self, n, nnz, ptr_d, idx_d, val_d, mval_d, b_d, x_d, **opt):
+        """A^T x = b with preconditioner M^T (the adjoint solve)."""
+        o = N.default_options(**opt)
+        info = N.SolveInfo()
+        self._check(self._L.dcu_bicgstab_transpose_d(self.h, n, nnz, _p(ptr_d), _p(idx_d), _p(val_d), _p(mval_d),
+                                                     _p(b_d), _p(x_d), C.byref(o), C.byref(info)))
+        return info
+
+    def sampled_outer_d(self, n, nnz, ptr_d, idx_d, u_d, v_d, alpha, out_d):
+        self._check(self._L.dcu_sampled_outer_d(self.h, n, nnz, _p(ptr_d), _p(idx_d), _p(u_d), _p(v_d),
+                                                float(alpha), _p(out_d)))
+
     def solve_d(self, n, nnz, ptr_d, idx_d, val_d, b_d, x_d, mval_d=None, **opt):
         o = N.default_options(**opt)
         bi, si = N.BuildInfo(), N.SolveInfo()

@@ -55,10 +55,10 @@ int resolve_range(Ctx* c, int n, const dcu_options* in, dcu_options* out) {
   return DCU_OK;
 }
 
-// Solver-side layout of A and M: SELL plan + values.
-int prepare_solve(Ctx* c, int n, int nnz, const int* ptr, const int* idx, const double* val, const double* mval,
-                  int precision, dcu::SellPlan* plan, const void** msell) {
-  DCU_TRY(dcu::sell_plan(c, n, nnz, ptr, idx, plan));
+// A's values (FP64) and M's (by form) in SELL order.
+int gather_values(Ctx* c, const dcu::SellPlan& pl, const double* val, const double* mval, int precision,
+                  const void** msell) {
+  const dcu::SellPlan* plan = &pl;
   const size_t slots = (size_t)(plan->slots > 0 ? plan->slots : 1);
   DCU_TRY(dcu::ensure(c, dcu::B_SELL_AVAL, sizeof(double) * slots));
   DCU_TRY(dcu::sell_gather_f64(c, *plan, val, dcu::bp<double>(c, dcu::B_SELL_AVAL)));
@@ -74,6 +74,13 @@ int prepare_solve(Ctx* c, int n, int nnz, const int* ptr, const int* idx, const 
   }
   *msell = c->buf[dcu::B_SELL_MVAL].p;
   return DCU_OK;
+}
+
+// Solver-side layout of A and M: SELL plan + values.
+int prepare_solve(Ctx* c, int n, int nnz, const int* ptr, const int* idx, const double* val, const double* mval,
+                  int precision, dcu::SellPlan* plan, const void** msell) {
+  DCU_TRY(dcu::sell_plan(c, n, nnz, ptr, idx, plan));
+  return gather_values(c, *plan, val, mval, precision, msell);
 }
 
 // Host uploads share one buffer: ptr | idx | val | b | x | mval.
@@ -377,6 +384,40 @@ int dcu_spai_solve_d(dcu_spai_ctx* c, int n, int nnz, const int* ptr, const int*
   } catch (const std::bad_alloc&) {
     return dcu::fail(c, DCU_ERR_ALLOC, "host allocation failed");
   }
+}
+
+int dcu_bicgstab_transpose_d(dcu_spai_ctx* c, int n, int nnz, const int* ptr, const int* idx, const double* val,
+                             const double* mval, const double* b, double* x, const dcu_options* opt,
+                             dcu_solve_info* info) {
+  int rc = check_matrix(c, n, nnz, ptr, idx, val);
+  if (rc) return rc;
+  if (!b || !x || (nnz > 0 && !mval)) return dcu::fail(c, DCU_ERR_ARG, "null vector or preconditioner");
+  dcu_options o;
+  if ((rc = resolve_range(c, n, opt, &o))) return rc;
+  try {
+    StreamScope scope(c);
+    DCU_TRY(dcu::validate_csc(c, n, nnz, ptr, idx));
+    // A's CSC arrays are the CSR arrays of A^T (and of M^T: same pattern)
+    dcu::SellPlan plan;
+    DCU_TRY(dcu::sell_plan_rows(c, n, nnz, ptr, idx, &plan));
+    const void* msell = nullptr;
+    DCU_TRY(gather_values(c, plan, val, mval, o.precision, &msell));
+    return dcu::bicgstab_solve(c, plan, dcu::bp<double>(c, dcu::B_SELL_AVAL), msell, b, x, &o, info);
+  } catch (const std::bad_alloc&) {
+    return dcu::fail(c, DCU_ERR_ALLOC, "host allocation failed");
+  }
+}
+
+int dcu_sampled_outer_d(dcu_spai_ctx* c, int n, int nnz, const int* ptr, const int* idx, const double* u,
+                        const double* v, double alpha, double* out) {
+  int rc = check_matrix(c, n, nnz, ptr, idx, idx);
+  if (rc) return rc;
+  if (!u || !v || (nnz > 0 && !out)) return dcu::fail(c, DCU_ERR_ARG, "null vector");
+  StreamScope scope(c);
+  DCU_TRY(dcu::validate_csc(c, n, nnz, ptr, idx));
+  DCU_TRY(dcu::sampled_outer(c, n, ptr, idx, u, v, alpha, out));
+  DCU_CUDA(c, cudaStreamSynchronize(c->stream));
+  return DCU_OK;
 }
 
 int dcu_profile_iteration_kernels(dcu_spai_ctx* c, int reps, float* ms_out) {

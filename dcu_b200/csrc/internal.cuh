@@ -138,6 +138,11 @@ int csr_from_csc(Ctx* c, int n, int nnz, const int* ptr, const int* idx, int* rp
                  int* rperm);
 int csr_values(Ctx* c, int nnz, const int* rperm, const double* val, double* rval);
 int sell_plan(Ctx* c, int n, int nnz, const int* ptr, const int* idx, SellPlan* plan);
+int sell_fill_from_csr(Ctx* c, int n, int nnz, const int* rptr, const int* rcol, const int* rperm, SellPlan* plan);
+int sell_plan_rows(Ctx* c, int n, int nnz, const int* rptr, const int* rcol, SellPlan* plan);
+// out[e] = alpha * u[idx[e]] * v[col(e)] on a CSC pattern
+int sampled_outer(Ctx* c, int n, const int* ptr, const int* idx, const double* u, const double* v, double alpha,
+                  double* out);
 // dst[slot] = (perm[slot] >= 0) ? src[perm[slot]] : 0, converted to the element type.
 int sell_gather_f64(Ctx* c, const SellPlan& p, const double* src, double* dst);
 int sell_gather_f32(Ctx* c, const SellPlan& p, const double* src, float* dst);

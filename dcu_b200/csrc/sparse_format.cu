@@ -266,7 +266,32 @@ __global__ void k_validate_csc(const int* __restrict__ ptr, const int* __restric
   if (b) atomicOr(bad, b);
 }
 
+__global__ void k_iota(int* __restrict__ out, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = i;
+}
+
+// out[e] = alpha * u[idx[e]] * v[j] for every entry e = (idx[e], j) of a CSC
+// pattern: the outer product u v^T sampled on the pattern (one warp per
+// column, lanes over the column's entries).
+__global__ void k_sampled_outer(const int* __restrict__ ptr, const int* __restrict__ idx, int n,
+                                const double* __restrict__ u, const double* __restrict__ v, double alpha,
+                                double* __restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < n; j += warps) {
+    const double vj = alpha * v[j];
+    for (int e = ptr[j] + lane; e < ptr[j + 1]; e += 32) out[e] = u[idx[e]] * vj;
+  }
+}
+
 }  // namespace
+
+int sampled_outer(Ctx* c, int n, const int* ptr, const int* idx, const double* u, const double* v, double alpha,
+                  double* out) {
+  k_sampled_outer<<<waves_grid(c, (long long)n * 32, 256, 8), 256, 0, c->stream>>>(ptr, idx, n, u, v, alpha, out);
+  DCU_LAUNCHED(c, "k_sampled_outer");
+  return DCU_OK;
+}
 
 int validate_csc(Ctx* c, int n, int nnz, const int* ptr, const int* idx) {
   DCU_TRY(ensure(c, B_ROWCNT, sizeof(int) * (size_t)(n + 1)));
@@ -332,6 +357,10 @@ int sell_plan(Ctx* c, int n, int nnz, const int* ptr, const int* idx, SellPlan* 
   int* rcol = bp<int>(c, B_RCOL);
   int* rperm = bp<int>(c, B_RPERM);
   DCU_TRY(csr_from_csc(c, n, nnz, ptr, idx, rptr, rcol, rperm));
+  return sell_fill_from_csr(c, n, nnz, rptr, rcol, rperm, plan);
+}
+
+int sell_fill_from_csr(Ctx* c, int n, int nnz, const int* rptr, const int* rcol, const int* rperm, SellPlan* plan) {
   int nslices = (n + 31) / 32;
   DCU_TRY(ensure(c, B_SELL_W, sizeof(int) * (size_t)(nslices + 1)));
   DCU_TRY(ensure(c, B_SELL_OFF, sizeof(long long) * (size_t)(nslices + 1)));
@@ -347,6 +376,7 @@ int sell_plan(Ctx* c, int n, int nnz, const int* ptr, const int* idx, SellPlan* 
   DCU_TRY(ensure(c, B_SELL_PERM, sizeof(int) * (size_t)(slots > 0 ? slots : 1)));
   int* sidx = bp<int>(c, B_SELL_IDX);
   int* sperm = bp<int>(c, B_SELL_PERM);
+  DCU_TRY(ensure(c, B_ROWCNT, sizeof(int) * (size_t)(n + 1)));
   int* maxdelta = bp<int>(c, B_ROWCNT);  // row counts are no longer needed
   DCU_CUDA(c, cudaMemsetAsync(maxdelta, 0, sizeof(int), c->stream));
   k_sell_fill<<<waves_grid(c, (long long)nslices * 32, 256, 8), 256, 0, c->stream>>>(rptr, rcol, rperm, n, nslices, off,
@@ -374,6 +404,20 @@ int sell_plan(Ctx* c, int n, int nnz, const int* ptr, const int* idx, SellPlan* 
   plan->idx = sidx;
   plan->perm = sperm;
   return DCU_OK;
+}
+
+// SELL-32 of the operator whose CSR is (rptr, rcol) as given, slot -> entry
+// position identity.  A CSC matrix read as CSR is its transpose, so
+// sell_plan_rows(A.ptr, A.idx) lays out A^T (and M^T, same pattern) for the
+// adjoint solve without any transpose.
+int sell_plan_rows(Ctx* c, int n, int nnz, const int* rptr, const int* rcol, SellPlan* plan) {
+  DCU_TRY(ensure(c, B_RPERM, sizeof(int) * (size_t)(nnz > 0 ? nnz : 1)));
+  int* rperm = bp<int>(c, B_RPERM);
+  if (nnz > 0) {
+    k_iota<<<waves_grid(c, nnz, 256, 8), 256, 0, c->stream>>>(rperm, nnz);
+    DCU_LAUNCHED(c, "k_iota");
+  }
+  return sell_fill_from_csr(c, n, nnz, rptr, rcol, rperm, plan);
 }
 
 int sell_gather_f64(Ctx* c, const SellPlan& p, const double* src, double* dst) { return sell_gather<double>(c, p, src, dst); }

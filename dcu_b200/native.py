@@ -64,6 +64,8 @@ SIGNATURES = {
     "dcu_csc_to_csr_noalloc_d": (_i, [_i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "dcu_bicgstab_d": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _OPT, C.POINTER(SolveInfo)]),
     "dcu_bicgstab_h": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _OPT, C.POINTER(SolveInfo)]),
+    "dcu_bicgstab_transpose_d": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _OPT, C.POINTER(SolveInfo)]),
+    "dcu_sampled_outer_d": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, C.c_double, _vp]),
     "dcu_spai_solve_d": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _OPT, _vp, C.POINTER(BuildInfo),
                               C.POINTER(SolveInfo)]),
     "dcu_spai_solve_h": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _OPT, _vp, C.POINTER(BuildInfo),

@@ -213,6 +213,21 @@ int dcu_bicgstab_h(dcu_spai_ctx* ctx, int n, int nnz, const int* ptr, const int*
                    const double* val, const double* mval, const double* b, double* x,
                    const dcu_options* opt, dcu_solve_info* info);
 
+/* The adjoint solve A^T x = b, right-preconditioned with M^T (same options
+ * and counter as dcu_bicgstab_d).  A's CSC arrays are read as the CSR arrays
+ * of A^T, so no transpose is formed.  No counterpart in the reference (the
+ * differentiation path of this library). */
+int dcu_bicgstab_transpose_d(dcu_spai_ctx* ctx, int n, int nnz, const int* ptr, const int* idx,
+                             const double* val, const double* mval, const double* b, double* x,
+                             const dcu_options* opt, dcu_solve_info* info);
+
+/* out[e] = alpha * u[idx[e]] * v[j] for every entry e of CSC column j: the
+ * outer product alpha u v^T sampled on A's pattern.  With u = lambda (adjoint
+ * solution), v = x and alpha = -1 this is dL/dA on A's nonzeros.  Device
+ * pointers.  No counterpart in the reference. */
+int dcu_sampled_outer_d(dcu_spai_ctx* ctx, int n, int nnz, const int* ptr, const int* idx,
+                        const double* u, const double* v, double alpha, double* out);
+
 /* The whole path: SPAI build of M on A's pattern, then BiCGSTAB.  mval
  * (optional) receives M (FP64, A's CSC order).  Device pointers. */
 int dcu_spai_solve_d(dcu_spai_ctx* ctx, int n, int nnz, const int* ptr, const int* idx,
