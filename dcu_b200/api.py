@@ -178,6 +178,20 @@ class Context:
         self._check(self._L.dcu_sampled_outer_d(self.h, n, nnz, _p(ptr_d), _p(idx_d), _p(u_d), _p(v_d),
                                                 float(alpha), _p(out_d)))
 
+    def batch_solve_d(self, sys_off_d, n, nnz, ptr_d, idx_d, val_d, B_d, X_d, mval_d=None, **opt):
+        """Independent diagonal-block systems x nrhs (B_d, X_d: n x nrhs).
+        Returns (iters[nsys, nrhs], status[nsys, nrhs], BuildInfo, SolveInfo)."""
+        o = N.default_options(**opt)
+        nsys = sys_off_d.numel() - 1
+        nrhs = B_d.shape[1]
+        iters = np.zeros(nsys * nrhs, dtype=np.int32)
+        status = np.zeros(nsys * nrhs, dtype=np.int32)
+        bi, si = N.BuildInfo(), N.SolveInfo()
+        self._check(self._L.dcu_batch_solve_d(self.h, nsys, _p(sys_off_d), n, nnz, _p(ptr_d), _p(idx_d),
+                                              _p(val_d), nrhs, _p(B_d), _p(X_d), C.byref(o), _p(mval_d),
+                                              _p(iters), _p(status), C.byref(bi), C.byref(si)))
+        return iters.reshape(nsys, nrhs), status.reshape(nsys, nrhs), bi, si
+
     def solve_d(self, n, nnz, ptr_d, idx_d, val_d, b_d, x_d, mval_d=None, **opt):
         o = N.default_options(**opt)
         bi, si = N.BuildInfo(), N.SolveInfo()

@@ -25,7 +25,7 @@ CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 HOST_CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["runtime.cu", "sparse_format.cu", "spai_build.cu", "bicgstab.cu", "capi.cu"]
+CU_SOURCES = ["runtime.cu", "sparse_format.cu", "spai_build.cu", "bicgstab.cu", "batched.cu", "capi.cu"]
 CXX_SOURCES = ["host_api.cpp", "mtx_io.cpp"]
 
 

@@ -1,0 +1,605 @@
+// Batched BiCGSTAB: many independent systems (the diagonal blocks of one
+// block-diagonal matrix) times R right-hand sides each, solved together.
+//
+// Every (system, right-hand side) pair runs the recurrences of
+// cublas2_pbicgstabv2 (include/bicgstab/bicgstab_solver.h:33-275) with its own
+// rho, alpha, omega, beta and stop test; pairs that converge are frozen (x no
+// longer changes) while the others continue.  Layout: A and M in SELL-32 over
+// all N rows; vectors row-major N x R, so one thread computes its row for all
+// R right-hand sides and every matrix entry read from HBM serves R products
+// (R contiguous doubles per gathered column).  Thread blocks are tiles of 256
+// rows inside one system; each dot product leaves one partial per tile and
+// the last tile of a system to finish sums that system's partials in tile
+// order (deterministic) and updates the system's scalars.
+#include <algorithm>
+
+#include "internal.cuh"
+
+namespace dcu {
+namespace {
+
+constexpr int BT = 256;           // rows per tile (= threads per block)
+constexpr int BT_WARPS = BT / 32;
+constexpr int BCHUNK = 8;         // iterations per graph launch
+
+struct BState {                   // per (system, rhs) pair, length S * R
+  double* rho;
+  double* alpha;
+  double* omega;
+  double* beta;
+  double* res;
+  double* thr;
+  double* bnorm;
+  int* active;                    // 1 while iterating
+  int* conv_it;                   // iteration counter when it stopped
+  int* status;                    // dcu_solve_status
+};
+
+struct BGlobal {
+  int it;                         // the reference's counter, shared by all pairs
+  int done;
+  int active_count;
+  int systems_done;               // systems finished in the current kernel
+  int pidx;
+  int maxiter;
+  int pad[2];
+};
+
+template <int R>
+struct BArgs {
+  int n, nsys, ntiles;
+  const int* sys_off;             // [nsys + 1]
+  const int* tile_sys;            // [ntiles]
+  const int* tile_row0;           // [ntiles]
+  const int* tile_off;            // [nsys + 1] first tile of each system
+  const long long* off;
+  const int* ix;
+  const double* aval;
+  const double* mval;
+  const double* b;
+  double* x;
+  double* r;
+  double* rs;
+  double* p0;
+  double* p1;
+  double* y;
+  double* ay;
+  double* s;
+  double* z;
+  double* az;
+  double* part;                   // [ntiles][3][R]
+  unsigned* cnt;                  // [nsys] tiles finished, per kernel
+  BState st;
+  BGlobal* g;
+};
+
+// out[q] = sum_k val * X[col][q], q < R, X row-major with R columns.
+template <int R, typename F>
+__device__ __forceinline__ void sell_row_multi(const long long* __restrict__ off, const double* __restrict__ val,
+                                               const int* __restrict__ ix, int row, F xf, double (&out)[R]) {
+#pragma unroll
+  for (int q = 0; q < R; ++q) out[q] = 0.0;
+  const int sl = row >> 5;
+  const long long o0 = __ldg(off + sl), o1 = __ldg(off + sl + 1);
+  const long long base = o0 + (row & 31);
+  const int w = (int)((o1 - o0) >> 5);
+  for (int k = 0; k < w; ++k) {
+    const long long qk = base + 32ll * k;
+    const double a = __ldcs(val + qk);
+    const int c = __ldcs(ix + qk);
+    double xv[R];
+    xf(c, xv);
+#pragma unroll
+    for (int q = 0; q < R; ++q) out[q] += a * xv[q];
+  }
+}
+
+template <int R>
+__device__ __forceinline__ void load_row(const double* __restrict__ v, int row, double (&o)[R]) {
+  const double2* p = reinterpret_cast<const double2*>(v + (size_t)row * R);
+#pragma unroll
+  for (int q = 0; q < R / 2; ++q) {
+    const double2 t = __ldg(p + q);
+    o[2 * q] = t.x;
+    o[2 * q + 1] = t.y;
+  }
+  if (R & 1) o[R - 1] = __ldg(v + (size_t)row * R + R - 1);
+}
+
+// Block sums of ND * R values per thread into part[tile]; the last tile of
+// the system to finish gets the system totals (tile order) in tot and true.
+template <int ND, int R>
+__device__ __forceinline__ bool system_reduce(double (&v)[ND][R], double* __restrict__ part, unsigned* cnt, int tile,
+                                              int t0, int t1, int sys, double (&tot)[ND][R]) {
+  __shared__ double red[ND * R][BT_WARPS];
+  __shared__ int amlast;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int d = 0; d < ND; ++d)
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      double xs = v[d][q];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) xs += __shfl_xor_sync(0xffffffffu, xs, o);
+      if (lane == 0) red[d * R + q][wid] = xs;
+    }
+  __syncthreads();
+  if (threadIdx.x < ND * R) {
+    double ssum = 0.0;
+#pragma unroll
+    for (int w = 0; w < BT_WARPS; ++w) ssum += red[threadIdx.x][w];
+    part[(size_t)tile * (3 * R) + threadIdx.x] = ssum;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned done = atomicAdd(&cnt[sys], 1u);
+    amlast = (done == (unsigned)(t1 - t0 - 1)) ? 1 : 0;
+  }
+  __syncthreads();
+  if (!amlast) return false;
+  __threadfence();
+  // thread j < ND * R sums slot j over the system's tiles in order
+  if (threadIdx.x < ND * R) {
+    double ssum = 0.0;
+    for (int t = t0; t < t1; ++t) ssum += __ldcg(part + (size_t)t * (3 * R) + threadIdx.x);
+    red[threadIdx.x][0] = ssum;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int d = 0; d < ND; ++d)
+#pragma unroll
+    for (int q = 0; q < R; ++q) tot[d][q] = red[d * R + q][0];
+  if (threadIdx.x == 0) cnt[sys] = 0u;
+  return true;
+}
+
+__device__ __forceinline__ bool g_finished(const BGlobal* g) { return *(volatile const int*)&g->done != 0; }
+
+// After a system's last tile updated its scalars: the last system overall
+// advances the shared counter and decides whether the batch is done.
+__device__ __forceinline__ void system_finished_step(BGlobal* g, int nsys, bool advance) {
+  __threadfence();
+  const int k = atomicAdd(&g->systems_done, 1);
+  if (k == nsys - 1) {
+    g->systems_done = 0;
+    if (advance) {
+      g->pidx ^= 1;
+      if (g->active_count <= 0) {
+        g->done = 1;
+      } else {
+        g->it += 1;
+        if (g->it >= g->maxiter) g->done = 1;
+      }
+    }
+  }
+}
+
+template <int R>
+__global__ void __launch_bounds__(BT) kb_init(BArgs<R> a, double tol, int tol_mode) {
+  const int tile = blockIdx.x, sys = a.tile_sys[tile];
+  const int row = a.tile_row0[tile] + threadIdx.x;
+  const bool valid = row < a.sys_off[sys + 1];
+  double v[3][R] = {};
+  if (valid) {
+    double ax[R], bb[R];
+    sell_row_multi<R>(a.off, a.aval, a.ix, row, [&](int c, double (&o)[R]) { load_row<R>(a.x, c, o); }, ax);
+    load_row<R>(a.b, row, bb);
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      const double rr = bb[q] + (-1.0) * ax[q];
+      const size_t i = (size_t)row * R + q;
+      a.r[i] = rr;
+      a.rs[i] = rr;
+      a.p0[i] = 0.0;
+      a.p1[i] = 0.0;
+      a.ay[i] = 0.0;
+      v[0][q] += rr * rr;   // (r*, r) = (r, r) at the start
+      v[1][q] += rr * rr;
+      v[2][q] += bb[q] * bb[q];
+    }
+  }
+  double tot[3][R];
+  if (system_reduce<3, R>(v, a.part, a.cnt, tile, a.tile_off[sys], a.tile_off[sys + 1], sys, tot) &&
+      threadIdx.x == 0) {
+    int live = 0;
+    for (int q = 0; q < R; ++q) {
+      const int i = sys * R + q;
+      a.st.rho[i] = tot[0][q];
+      a.st.res[i] = sqrt(tot[1][q]);
+      a.st.bnorm[i] = sqrt(tot[2][q]);
+      a.st.thr[i] = (tol_mode == DCU_TOL_REL) ? tol * a.st.bnorm[i] : tol;
+      a.st.alpha[i] = 0.0;
+      a.st.omega[i] = 1.0;
+      a.st.beta[i] = 0.0;
+      const bool run = a.st.res[i] != 0.0 && a.g->maxiter > 1;
+      a.st.active[i] = run ? 1 : 0;
+      a.st.conv_it[i] = 1;
+      a.st.status[i] = run ? -1 : (a.st.res[i] == 0.0 ? DCU_SOLVE_CONVERGED : DCU_SOLVE_MAXITER);
+      live += run ? 1 : 0;
+    }
+    atomicAdd(&a.g->active_count, live);
+    system_finished_step(a.g, a.nsys, false);
+  }
+}
+
+// K1: p = r + beta (p - omega ay) at gathered columns; y = M p
+template <int R>
+__global__ void __launch_bounds__(BT) kb_py(BArgs<R> a) {
+  if (g_finished(a.g)) return;
+  const int tile = blockIdx.x, sys = a.tile_sys[tile];
+  const int row = a.tile_row0[tile] + threadIdx.x;
+  if (row >= a.sys_off[sys + 1]) return;
+  double beta[R], omega[R];
+#pragma unroll
+  for (int q = 0; q < R; ++q) {
+    beta[q] = a.st.beta[sys * R + q];
+    omega[q] = a.st.omega[sys * R + q];
+  }
+  const int pidx = a.g->pidx;
+  const double* pold = pidx ? a.p1 : a.p0;
+  double* pnew = pidx ? a.p0 : a.p1;
+  auto pf = [&](int c, double (&o)[R]) {
+    double rr[R], pp[R], yy[R];
+    load_row<R>(a.r, c, rr);
+    load_row<R>(pold, c, pp);
+    load_row<R>(a.ay, c, yy);
+#pragma unroll
+    for (int q = 0; q < R; ++q) o[q] = rr[q] + beta[q] * (pp[q] - omega[q] * yy[q]);
+  };
+  double yv[R], pv[R];
+  sell_row_multi<R>(a.off, a.mval, a.ix, row, pf, yv);
+  pf(row, pv);
+#pragma unroll
+  for (int q = 0; q < R; ++q) {
+    pnew[(size_t)row * R + q] = pv[q];
+    a.y[(size_t)row * R + q] = yv[q];
+  }
+}
+
+// K2: ay = A y; alpha = rho / (r*, ay)
+template <int R>
+__global__ void __launch_bounds__(BT) kb_ay(BArgs<R> a) {
+  if (g_finished(a.g)) return;
+  const int tile = blockIdx.x, sys = a.tile_sys[tile];
+  const int row = a.tile_row0[tile] + threadIdx.x;
+  double v[1][R] = {};
+  if (row < a.sys_off[sys + 1]) {
+    double ayv[R], rsv[R];
+    sell_row_multi<R>(a.off, a.aval, a.ix, row, [&](int c, double (&o)[R]) { load_row<R>(a.y, c, o); }, ayv);
+    load_row<R>(a.rs, row, rsv);
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      a.ay[(size_t)row * R + q] = ayv[q];
+      v[0][q] += rsv[q] * ayv[q];
+    }
+  }
+  double tot[1][R];
+  if (system_reduce<1, R>(v, a.part, a.cnt, tile, a.tile_off[sys], a.tile_off[sys + 1], sys, tot) &&
+      threadIdx.x == 0) {
+    for (int q = 0; q < R; ++q) {
+      const int i = sys * R + q;
+      if (!a.st.active[i]) continue;
+      const double alpha = a.st.rho[i] / tot[0][q];
+      a.st.alpha[i] = alpha;
+      if (tot[0][q] == 0.0 || !isfinite(alpha)) {
+        a.st.active[i] = 0;
+        a.st.status[i] = DCU_SOLVE_BREAKDOWN;
+        a.st.alpha[i] = a.st.omega[i] = a.st.beta[i] = 0.0;
+        atomicSub(&a.g->active_count, 1);
+      }
+    }
+    system_finished_step(a.g, a.nsys, false);
+  }
+}
+
+// K3: s = r - alpha ay (on the fly at gathered columns); z = M s
+template <int R>
+__global__ void __launch_bounds__(BT) kb_sz(BArgs<R> a) {
+  if (g_finished(a.g)) return;
+  const int tile = blockIdx.x, sys = a.tile_sys[tile];
+  const int row = a.tile_row0[tile] + threadIdx.x;
+  if (row >= a.sys_off[sys + 1]) return;
+  double nalpha[R];
+#pragma unroll
+  for (int q = 0; q < R; ++q) nalpha[q] = -1.0 * a.st.alpha[sys * R + q];
+  auto sf = [&](int c, double (&o)[R]) {
+    double rr[R], yy[R];
+    load_row<R>(a.r, c, rr);
+    load_row<R>(a.ay, c, yy);
+#pragma unroll
+    for (int q = 0; q < R; ++q) o[q] = rr[q] + nalpha[q] * yy[q];
+  };
+  double zv[R], sv[R];
+  sell_row_multi<R>(a.off, a.mval, a.ix, row, sf, zv);
+  sf(row, sv);
+#pragma unroll
+  for (int q = 0; q < R; ++q) {
+    a.s[(size_t)row * R + q] = sv[q];
+    a.z[(size_t)row * R + q] = zv[q];
+  }
+}
+
+// K4: az = A z; omega = (az, s) / (az, az)
+template <int R>
+__global__ void __launch_bounds__(BT) kb_az(BArgs<R> a) {
+  if (g_finished(a.g)) return;
+  const int tile = blockIdx.x, sys = a.tile_sys[tile];
+  const int row = a.tile_row0[tile] + threadIdx.x;
+  double v[2][R] = {};
+  if (row < a.sys_off[sys + 1]) {
+    double azv[R], sv[R];
+    sell_row_multi<R>(a.off, a.aval, a.ix, row, [&](int c, double (&o)[R]) { load_row<R>(a.z, c, o); }, azv);
+    load_row<R>(a.s, row, sv);
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      a.az[(size_t)row * R + q] = azv[q];
+      v[0][q] += azv[q] * sv[q];
+      v[1][q] += azv[q] * azv[q];
+    }
+  }
+  double tot[2][R];
+  if (system_reduce<2, R>(v, a.part, a.cnt, tile, a.tile_off[sys], a.tile_off[sys + 1], sys, tot) &&
+      threadIdx.x == 0) {
+    for (int q = 0; q < R; ++q) {
+      const int i = sys * R + q;
+      if (!a.st.active[i]) continue;
+      const double omega = tot[0][q] / tot[1][q];
+      a.st.omega[i] = omega;
+      if (tot[1][q] == 0.0 || omega == 0.0 || !isfinite(omega)) {
+        a.st.active[i] = 0;
+        a.st.status[i] = DCU_SOLVE_BREAKDOWN;
+        a.st.alpha[i] = a.st.omega[i] = a.st.beta[i] = 0.0;
+        atomicSub(&a.g->active_count, 1);
+      }
+    }
+    system_finished_step(a.g, a.nsys, false);
+  }
+}
+
+// K5: x += alpha y + omega z (active pairs); r = s - omega az; rho, beta, ||r||
+template <int R>
+__global__ void __launch_bounds__(BT) kb_xr(BArgs<R> a) {
+  if (g_finished(a.g)) return;
+  const int tile = blockIdx.x, sys = a.tile_sys[tile];
+  const int row = a.tile_row0[tile] + threadIdx.x;
+  double v[2][R] = {};
+  if (row < a.sys_off[sys + 1]) {
+    double yv[R], zv[R], sv[R], azv[R], rsv[R], xv[R];
+    load_row<R>(a.y, row, yv);
+    load_row<R>(a.z, row, zv);
+    load_row<R>(a.s, row, sv);
+    load_row<R>(a.az, row, azv);
+    load_row<R>(a.rs, row, rsv);
+    load_row<R>(a.x, row, xv);
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      const int i = sys * R + q;
+      const double alpha = a.st.alpha[i], omega = a.st.omega[i];
+      if (a.st.active[i]) {
+        double t = xv[q] + alpha * yv[q];
+        t = t + omega * zv[q];
+        a.x[(size_t)row * R + q] = t;
+      }
+      const double rn = sv[q] + (-1.0 * omega) * azv[q];
+      a.r[(size_t)row * R + q] = rn;
+      v[0][q] += rsv[q] * rn;
+      v[1][q] += rn * rn;
+    }
+  }
+  double tot[2][R];
+  if (system_reduce<2, R>(v, a.part, a.cnt, tile, a.tile_off[sys], a.tile_off[sys + 1], sys, tot) &&
+      threadIdx.x == 0) {
+    const int it = a.g->it;
+    for (int q = 0; q < R; ++q) {
+      const int i = sys * R + q;
+      if (!a.st.active[i]) continue;
+      const double rho_new = tot[0][q];
+      const double beta = (rho_new / a.st.rho[i]) * (a.st.alpha[i] / a.st.omega[i]);
+      a.st.rho[i] = rho_new;
+      a.st.beta[i] = beta;
+      a.st.res[i] = sqrt(tot[1][q]);
+      a.st.conv_it[i] = it;
+      if (!isfinite(a.st.res[i]) || !isfinite(beta) || rho_new == 0.0) {
+        a.st.active[i] = 0;
+        a.st.status[i] = DCU_SOLVE_BREAKDOWN;
+      } else if (a.st.res[i] < a.st.thr[i]) {
+        a.st.active[i] = 0;
+        a.st.status[i] = DCU_SOLVE_CONVERGED;
+      } else if (it + 1 >= a.g->maxiter) {
+        a.st.status[i] = DCU_SOLVE_MAXITER;
+        a.st.conv_it[i] = it + 1;
+      }
+      if (!a.st.active[i]) {
+        a.st.alpha[i] = a.st.omega[i] = a.st.beta[i] = 0.0;
+        atomicSub(&a.g->active_count, 1);
+      }
+    }
+    system_finished_step(a.g, a.nsys, true);
+  }
+}
+
+__global__ void kb_check_blocks(const int* __restrict__ ptr, const int* __restrict__ idx, const int* __restrict__ sys_off,
+                                int nsys, int n, int* __restrict__ bad) {
+  // every column's rows lie in its own diagonal block
+  for (int s = blockIdx.x; s < nsys; s += gridDim.x) {
+    const int c0 = sys_off[s], c1 = sys_off[s + 1];
+    if (threadIdx.x == 0 && (c1 < c0 || c0 < 0 || c1 > n)) atomicOr(bad, 1);
+    for (int c = c0 + threadIdx.x; c < c1 && c0 >= 0 && c1 <= n; c += blockDim.x)
+      for (int e = ptr[c]; e < ptr[c + 1]; ++e)
+        if (idx[e] < c0 || idx[e] >= c1) atomicOr(bad, 2);
+  }
+}
+
+template <int R>
+int run_batch(Ctx* c, int nsys, const int* sys_off_d, const SellPlan& plan, const double* aval, const double* mval,
+              const double* B, double* X, const dcu_options* opt, int* iters_h, int* status_h,
+              dcu_solve_info* info) {
+  const int n = plan.n;
+  // host copy of the system offsets -> tiles
+  std::vector<int> so(nsys + 1);
+  DCU_CUDA(c, cudaMemcpyAsync(so.data(), sys_off_d, sizeof(int) * (nsys + 1), cudaMemcpyDeviceToHost, c->stream));
+  DCU_CUDA(c, cudaStreamSynchronize(c->stream));
+  std::vector<int> tsys, trow, toff(nsys + 1, 0);
+  for (int s = 0; s < nsys; ++s) {
+    toff[s] = (int)tsys.size();
+    for (int r0 = so[s]; r0 < so[s + 1]; r0 += BT) {
+      tsys.push_back(s);
+      trow.push_back(r0);
+    }
+  }
+  toff[nsys] = (int)tsys.size();
+  const int ntiles = (int)tsys.size();
+  if (ntiles == 0) return fail(c, DCU_ERR_ARG, "empty batch");
+  auto al = [](size_t v) { return (v + 255) & ~(size_t)255; };
+  const size_t vec = al(sizeof(double) * (size_t)n * R);
+  const size_t pairs = (size_t)nsys * R;
+  const size_t small = al(sizeof(int) * (2 * (size_t)ntiles + nsys + 1)) + al(sizeof(unsigned) * nsys) +
+                       al(sizeof(double) * 3 * R * (size_t)ntiles) + al(sizeof(double) * 7 * pairs) +
+                       al(sizeof(int) * 3 * pairs) + al(sizeof(BGlobal));
+  DCU_TRY(ensure(c, B_VEC, 9 * vec + small));
+  char* p = bp<char>(c, B_VEC);
+  BArgs<R> a{};
+  a.n = n;
+  a.nsys = nsys;
+  a.ntiles = ntiles;
+  a.sys_off = sys_off_d;
+  a.off = plan.off;
+  a.ix = plan.idx;
+  a.aval = aval;
+  a.mval = mval;
+  a.b = B;
+  a.x = X;
+  double* vecs[9];
+  for (int i = 0; i < 9; ++i) vecs[i] = reinterpret_cast<double*>(p + i * vec);
+  a.r = vecs[0]; a.rs = vecs[1]; a.p0 = vecs[2]; a.p1 = vecs[3]; a.y = vecs[4];
+  a.ay = vecs[5]; a.s = vecs[6]; a.z = vecs[7]; a.az = vecs[8];
+  char* q = p + 9 * vec;
+  int* tiles = reinterpret_cast<int*>(q);
+  a.tile_sys = tiles;
+  a.tile_row0 = tiles + ntiles;
+  a.tile_off = tiles + 2 * ntiles;
+  q += al(sizeof(int) * (2 * (size_t)ntiles + nsys + 1));
+  a.cnt = reinterpret_cast<unsigned*>(q);
+  q += al(sizeof(unsigned) * nsys);
+  a.part = reinterpret_cast<double*>(q);
+  q += al(sizeof(double) * 3 * R * (size_t)ntiles);
+  double* dst = reinterpret_cast<double*>(q);
+  a.st.rho = dst; a.st.alpha = dst + pairs; a.st.omega = dst + 2 * pairs; a.st.beta = dst + 3 * pairs;
+  a.st.res = dst + 4 * pairs; a.st.thr = dst + 5 * pairs; a.st.bnorm = dst + 6 * pairs;
+  q += al(sizeof(double) * 7 * pairs);
+  int* ist = reinterpret_cast<int*>(q);
+  a.st.active = ist; a.st.conv_it = ist + pairs; a.st.status = ist + 2 * pairs;
+  q += al(sizeof(int) * 3 * pairs);
+  a.g = reinterpret_cast<BGlobal*>(q);
+  DCU_CUDA(c, cudaMemcpyAsync(tiles, tsys.data(), sizeof(int) * ntiles, cudaMemcpyHostToDevice, c->stream));
+  DCU_CUDA(c, cudaMemcpyAsync(tiles + ntiles, trow.data(), sizeof(int) * ntiles, cudaMemcpyHostToDevice, c->stream));
+  DCU_CUDA(c, cudaMemcpyAsync(tiles + 2 * ntiles, toff.data(), sizeof(int) * (nsys + 1), cudaMemcpyHostToDevice,
+                              c->stream));
+  DCU_CUDA(c, cudaMemsetAsync(a.cnt, 0, sizeof(unsigned) * nsys, c->stream));
+  const int maxiter = opt->maxiter > 0 ? opt->maxiter : n;
+  BGlobal g0{};
+  g0.it = 1;
+  g0.maxiter = maxiter;
+  DCU_CUDA(c, cudaMemcpyAsync(a.g, &g0, sizeof(BGlobal), cudaMemcpyHostToDevice, c->stream));
+  DCU_CUDA(c, cudaEventRecord(c->ev[0], c->stream));
+  kb_init<R><<<ntiles, BT, 0, c->stream>>>(a, opt->tol, opt->tol_mode);
+  DCU_LAUNCHED(c, "kb_init");
+  // the first iteration starts with p = r: beta = 0 and p, ay zero-filled
+  std::vector<const void*> key = {(const void*)&kb_py<R>, plan.off, aval, mval, B, X, p, (const void*)(intptr_t)n,
+                                  (const void*)(intptr_t)nsys, (const void*)(intptr_t)ntiles};
+  GraphSlot* ge = nullptr;
+  for (auto& e : c->graphs)
+    if (e.key == key) ge = &e;
+  if (!ge) {
+    cudaGraph_t gr = nullptr;
+    DCU_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    for (int i = 0; i < BCHUNK; ++i) {
+      kb_py<R><<<ntiles, BT, 0, c->stream>>>(a);
+      kb_ay<R><<<ntiles, BT, 0, c->stream>>>(a);
+      kb_sz<R><<<ntiles, BT, 0, c->stream>>>(a);
+      kb_az<R><<<ntiles, BT, 0, c->stream>>>(a);
+      kb_xr<R><<<ntiles, BT, 0, c->stream>>>(a);
+    }
+    cudaError_t e = cudaStreamEndCapture(c->stream, &gr);
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture", __FILE__, __LINE__);
+    GraphSlot ne;
+    ne.key = key;
+    ne.nodes = 5 * BCHUNK;
+    e = cudaGraphInstantiate(&ne.exec, gr, 0);
+    cudaGraphDestroy(gr);
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaGraphInstantiate", __FILE__, __LINE__);
+    if (c->graphs.size() >= 8) {
+      cudaGraphExecDestroy(c->graphs.front().exec);
+      c->graphs.erase(c->graphs.begin());
+    }
+    c->graphs.push_back(ne);
+    ge = &c->graphs.back();
+  }
+  int* flag = reinterpret_cast<int*>(reinterpret_cast<char*>(c->pinned) + 1024);
+  const long long max_chunks = (long long)maxiter / BCHUNK + 4;
+  for (long long i = 0;; ++i) {
+    if (i > max_chunks) return fail(c, DCU_ERR_CUDA, "batched solver did not terminate");
+    DCU_CUDA(c, cudaGraphLaunch(ge->exec, c->stream));
+    c->launches += ge->nodes;
+    DCU_CUDA(c, cudaMemcpyAsync(flag + (i & 1), &a.g->done, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    DCU_CUDA(c, cudaEventRecord(c->ev[2 + (i & 1)], c->stream));
+    if (i > 0) {
+      DCU_CUDA(c, cudaEventSynchronize(c->ev[2 + ((i - 1) & 1)]));
+      if (flag[(i - 1) & 1]) break;
+    }
+  }
+  DCU_CUDA(c, cudaEventRecord(c->ev[1], c->stream));
+  DCU_CUDA(c, cudaMemcpyAsync(iters_h, a.st.conv_it, sizeof(int) * pairs, cudaMemcpyDeviceToHost, c->stream));
+  DCU_CUDA(c, cudaMemcpyAsync(status_h, a.st.status, sizeof(int) * pairs, cudaMemcpyDeviceToHost, c->stream));
+  BGlobal gh;
+  DCU_CUDA(c, cudaMemcpyAsync(&gh, a.g, sizeof(BGlobal), cudaMemcpyDeviceToHost, c->stream));
+  DCU_CUDA(c, cudaStreamSynchronize(c->stream));
+  int worst = DCU_SOLVE_CONVERGED;
+  for (size_t i = 0; i < pairs; ++i) {
+    if (status_h[i] < 0) {   // still running when the shared counter hit maxiter
+      status_h[i] = DCU_SOLVE_MAXITER;
+      iters_h[i] = gh.it;
+    }
+    worst = std::max(worst, status_h[i]);
+  }
+  if (info) {
+    info->iters = gh.it;
+    info->status = worst;
+    info->replacements = 0;
+    info->res = info->true_res = info->bnorm = 0.0;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+    info->ms = ms;
+  }
+  return DCU_OK;
+}
+
+}  // namespace
+
+int check_blocks(Ctx* c, int n, const int* ptr, const int* idx, int nsys, const int* sys_off) {
+  DCU_TRY(ensure(c, B_STATS, sizeof(int) * 16));
+  int* bad = bp<int>(c, B_STATS);
+  DCU_CUDA(c, cudaMemsetAsync(bad, 0, sizeof(int), c->stream));
+  kb_check_blocks<<<std::min(nsys, 4096), 128, 0, c->stream>>>(ptr, idx, sys_off, nsys, n, bad);
+  DCU_LAUNCHED(c, "kb_check_blocks");
+  int h = 0;
+  DCU_CUDA(c, cudaMemcpyAsync(&h, bad, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  DCU_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (h) return fail(c, DCU_ERR_ARG, "matrix is not block diagonal with respect to the system offsets (%d)", h);
+  return DCU_OK;
+}
+
+int batch_solve(Ctx* c, int nsys, const int* sys_off, const SellPlan& plan, const double* aval, const double* mval,
+                int nrhs, const double* B, double* X, const dcu_options* opt, int* iters, int* status,
+                dcu_solve_info* info) {
+  switch (nrhs) {
+    case 1: return run_batch<1>(c, nsys, sys_off, plan, aval, mval, B, X, opt, iters, status, info);
+    case 2: return run_batch<2>(c, nsys, sys_off, plan, aval, mval, B, X, opt, iters, status, info);
+    case 4: return run_batch<4>(c, nsys, sys_off, plan, aval, mval, B, X, opt, iters, status, info);
+    case 8: return run_batch<8>(c, nsys, sys_off, plan, aval, mval, B, X, opt, iters, status, info);
+    default: return fail(c, DCU_ERR_ARG, "nrhs must be 1, 2, 4 or 8 (got %d)", nrhs);
+  }
+}
+
+}  // namespace dcu

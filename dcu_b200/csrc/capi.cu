@@ -420,6 +420,44 @@ int dcu_sampled_outer_d(dcu_spai_ctx* c, int n, int nnz, const int* ptr, const i
   return DCU_OK;
 }
 
+int dcu_batch_solve_d(dcu_spai_ctx* c, int nsys, const int* sys_off, int n, int nnz, const int* ptr, const int* idx,
+                      const double* val, int nrhs, const double* B, double* X, const dcu_options* opt, double* mval,
+                      int* iters, int* status, dcu_build_info* binfo, dcu_solve_info* sinfo) {
+  int rc = check_matrix(c, n, nnz, ptr, idx, val);
+  if (rc) return rc;
+  if (nsys <= 0 || !sys_off || !B || !X || !iters || !status)
+    return dcu::fail(c, DCU_ERR_ARG, "invalid batch arguments");
+  dcu_options o;
+  if ((rc = resolve_range(c, n, opt, &o))) return rc;
+  if (o.col_start != 0 || o.col_end != n) return dcu::fail(c, DCU_ERR_ARG, "a batch builds every column");
+  if (o.precision != DCU_PREC_FP64) return dcu::fail(c, DCU_ERR_ARG, "the batched solver runs the FP64 form");
+  try {
+    StreamScope scope(c);
+    DCU_TRY(dcu::validate_csc(c, n, nnz, ptr, idx));
+    DCU_TRY(dcu::check_blocks(c, n, ptr, idx, nsys, sys_off));
+    double* m = mval;
+    if (!m) {
+      DCU_TRY(dcu::ensure(c, dcu::B_MVAL, sizeof(double) * (size_t)(nnz > 0 ? nnz : 1)));
+      m = dcu::bp<double>(c, dcu::B_MVAL);
+    }
+    // one build over all columns: M of a block-diagonal A is block diagonal
+    dcu_build_info bl{};
+    DCU_CUDA(c, cudaEventRecord(c->ev[0], c->stream));
+    DCU_TRY(dcu::spai_build(c, n, nnz, ptr, idx, val, &o, m, nullptr, &bl));
+    DCU_CUDA(c, cudaEventRecord(c->ev[1], c->stream));
+    DCU_CUDA(c, cudaEventSynchronize(c->ev[1]));
+    cudaEventElapsedTime(&bl.ms, c->ev[0], c->ev[1]);
+    if (binfo) *binfo = bl;
+    dcu::SellPlan plan;
+    const void* msell = nullptr;
+    DCU_TRY(prepare_solve(c, n, nnz, ptr, idx, val, m, DCU_PREC_FP64, &plan, &msell));
+    return dcu::batch_solve(c, nsys, sys_off, plan, dcu::bp<double>(c, dcu::B_SELL_AVAL), (const double*)msell,
+                            nrhs, B, X, &o, iters, status, sinfo);
+  } catch (const std::bad_alloc&) {
+    return dcu::fail(c, DCU_ERR_ALLOC, "host allocation failed");
+  }
+}
+
 int dcu_profile_iteration_kernels(dcu_spai_ctx* c, int reps, float* ms_out) {
   if (!c || !ms_out) return DCU_ERR_ARG;
   StreamScope scope(c);

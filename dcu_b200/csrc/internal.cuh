@@ -165,6 +165,12 @@ int spai_pattern(Ctx* c, int n, const int* ptr, const int* idx, int col_start, i
 int bicgstab_solve(Ctx* c, const SellPlan& plan, const double* aval_sell, const void* mval_sell,
                    const double* b, double* x, const dcu_options* opt, dcu_solve_info* info);
 void release_graphs(Ctx* c);
+
+// Batched systems (diagonal blocks [sys_off[s], sys_off[s+1]) of one matrix).
+int check_blocks(Ctx* c, int n, const int* ptr, const int* idx, int nsys, const int* sys_off);
+int batch_solve(Ctx* c, int nsys, const int* sys_off, const SellPlan& plan, const double* aval, const double* mval,
+                int nrhs, const double* B, double* X, const dcu_options* opt, int* iters, int* status,
+                dcu_solve_info* info);
 int profile_iteration(Ctx* c, int reps, float* ms);
 
 // grid size for grid-stride kernels: whole waves of `per_sm` blocks

@@ -239,6 +239,23 @@ int dcu_spai_solve_h(dcu_spai_ctx* ctx, int n, int nnz, const int* ptr, const in
                      const double* val, const double* b, double* x, const dcu_options* opt,
                      double* mval, dcu_build_info* binfo, dcu_solve_info* sinfo);
 
+/* Batched solve of independent systems: the diagonal blocks
+ * [sys_off[s], sys_off[s+1]) of one block-diagonal CSC matrix (device
+ * sys_off, int32, nsys + 1 entries, sys_off[0] = 0, sys_off[nsys] = n), each
+ * with nrhs (1, 2, 4 or 8) right-hand sides.  B and X are device, row-major
+ * n x nrhs; X holds x0 on entry.  One SPAI build covers every column (M of a
+ * block-diagonal A is block diagonal); then one BiCGSTAB iteration stream
+ * advances all (system, rhs) pairs, each with its own scalars and stop test,
+ * freezing converged pairs.  iters / status (host, nsys * nrhs, pair
+ * s * nrhs + q) receive each pair's counter and dcu_solve_status; sinfo->iters
+ * is the shared counter at exit.  FP64 form only (opt->precision 0);
+ * opt->ls_method applies to the build.  Fails with DCU_ERR_ARG when an entry
+ * lies outside its diagonal block. */
+int dcu_batch_solve_d(dcu_spai_ctx* ctx, int nsys, const int* sys_off, int n, int nnz, const int* ptr,
+                      const int* idx, const double* val, int nrhs, const double* B, double* X,
+                      const dcu_options* opt, double* mval, int* iters, int* status,
+                      dcu_build_info* binfo, dcu_solve_info* sinfo);
+
 /* Diagnostic timing: re-launch each of the five fused iteration kernels of
  * the last solve on this context (K1 p/y = M p, K2 A y + (r*,Ay), K3 s/z = M s,
  * K4 A z + dots, K5 x/r update + dots) `reps` times on that solve's buffers
