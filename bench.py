@@ -6,16 +6,21 @@ b = A x_true with x_true ~ N(0,1) (seeded), x0 = 0, SPAI pattern = pattern of
 A, BiCGSTAB to ||b - A x|| < 1e-8 ||b|| (verified in FP64), maxiter 1000.
 Synthetic seeded data; the reference publishes no number for it.
 
-  value  ms of the headline form (mixed precision M + FP32 least squares,
-         --form) with A, b resident in HBM
+  value  ms of the headline form (--form, default m_bf16: FP32 least squares
+         on the thread-per-column path, M stored as BF16 with 16-bit column
+         deltas, FP64 Krylov vectors) with A, b resident in HBM
   e2e    the same through the host-buffer C entry point dcu_spai_solve_h:
          pinned host A, b, x0 -> device, solve, x -> host, per step
   plain_fp64_ms  the plain FP64 form on the same inputs (the north star's
          comparison), measured in the same run
 
 python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                [--workload cd3d128|batch512|grad512]
 Under torchrun each rank solves its own copy (replicas; weak scaling, no
-collective on the data path); ms is the max over ranks.
+collective on the data path); ms is the max over ranks.  batch512 (512
+stencil systems x 8 right-hand sides, batched solver) and grad512 (512^2
+variable-coefficient diffusion, forward solve + adjoint gradient) print their
+own lines; the default workload is the headline.
 """
 from __future__ import annotations
 
@@ -145,13 +150,86 @@ def run_reference(args, rank, world):
     return 0
 
 
+def run_extra(args, rank, world):
+    """batch512 / grad512 on one GPU (rank 0)."""
+    if rank != 0:
+        return 0
+    import torch
+
+    from dcu_b200 import native as N
+    from dcu_b200 import workloads as W
+    from dcu_b200.api import Context
+
+    dev = torch.device("cuda", 0)
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    ctx = Context(0)
+    stream = torch.cuda.current_stream(dev)
+    ctx.set_stream(stream.cuda_stream)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    if args.workload == "batch512":
+        bt = W.batch_systems()
+        A = bt.A
+        off, ptr, idx, val, B = d(bt.offsets.astype(np.int32)), d(A.ptr), d(A.idx), d(A.val), d(bt.B)
+        X = torch.zeros((A.n, bt.B.shape[1]), dtype=torch.float64, device=dev)
+
+        def step():
+            X.zero_()
+            return ctx.batch_solve_d(off, A.n, A.nnz, ptr, idx, val, B, X, ls_method=N.LS_NORMAL_EQ)
+        metric = "batched SPAI build+BiCGSTAB ms (512 systems x 8 rhs, each to 1e-8 rel.)"
+        cfg = {"workload": "512 stencil systems (2D 5-pt / 3D 7-pt, n log-uniform 1e3..5e4, Pe U[0,50]) x 8 "
+                           "rhs U[-1,1], FP64, one build + one batched iteration stream", "n": A.n, "nnz": A.nnz,
+               "systems": int(len(bt.offsets) - 1), "rhs": int(bt.B.shape[1])}
+    else:
+        from dcu_b200.autograd import spai_solve
+
+        Av = W.varcoef2d(512, seed=5)
+        rng = np.random.Generator(np.random.PCG64(5))
+        b, xt = d(rng.standard_normal(Av.n)), d(rng.standard_normal(Av.n))
+        p2, i2, v2 = d(Av.ptr), d(Av.idx), d(Av.val)
+
+        def step():
+            vv = v2.clone().requires_grad_(True)
+            bb = b.clone().requires_grad_(True)
+            x = spai_solve(vv, bb, p2, i2, ctx, maxiter=3000)
+            L = ((x - xt) ** 2).sum()
+            L.backward()
+            return vv.grad, bb.grad
+        metric = "forward SPAI+BiCGSTAB + adjoint gradient ms (512^2 variable-coefficient diffusion, FP64)"
+        cfg = {"workload": "varcoef2d 512^2, kappa = exp(GRF, corr 16, var 1), small upwind advection; "
+                           "L = ||x - x_t||^2; dL/db and dL/dA on A's pattern", "n": Av.n, "nnz": Av.nnz}
+    for _ in range(args.warmup):
+        out = step()
+    torch.cuda.synchronize(dev)
+    ms = []
+    for i in range(args.steps):
+        flush.fill_(float(i))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = step()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        ms.append(e0.elapsed_time(e1))
+    if args.workload == "batch512":
+        it, st, bi, si = out
+        cfg.update({"shared_iters": si.iters, "pair_iters_mean": float(it.mean()), "pair_iters_max": int(it.max()),
+                    "all_converged": bool((st == 0).all()), "build_ms": round(bi.ms, 3)})
+    v = statistics.mean(ms)
+    print(json.dumps({"metric": metric, "value": round(v, 3), "unit": "ms", "n_gpus": 1, "steps": args.steps,
+                      "warmup": args.warmup, "ms_per_step": round(v, 3), "higher_is_better": False,
+                      "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg}),
+          flush=True)
+    ctx.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="mixed_bf16", choices=list(FORMS))
+    ap.add_argument("--form", default="m_bf16", choices=list(FORMS))
+    ap.add_argument("--workload", default="cd3d128", choices=["cd3d128", "batch512", "grad512"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-only", action="store_true", help="one plain + one headline solve, no timing loop")
     args = ap.parse_args()
@@ -163,6 +241,8 @@ def main():
 
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.workload != "cd3d128":
+        return run_extra(args, rank, world)
 
     import torch
 
@@ -225,9 +305,20 @@ def main():
     clocks = clk.summary()
     ms_plain, inf_plain, _ = timed(FORMS["fp64"], steps)
     barrier()
+    x_plain = x.cpu().numpy()
 
-    xh = x.cpu().numpy()  # last plain solve
-    relres_plain = float(np.linalg.norm(b_h - A.matvec(xh)) / np.linalg.norm(b_h))
+    # ablation: every precision form on the same inputs (same timing rules)
+    forms = {}
+    if not args.profile_only:
+        for name, f in FORMS.items():
+            for _ in range(2):
+                solve(f)
+            msf, inff, _ = timed(f, steps)
+            forms[name] = {"ms": round(statistics.mean(msf), 3), "iters": inff[-1][1].iters,
+                           "build_ms": round(inff[-1][0].ms, 3)}
+        barrier()
+
+    relres_plain = float(np.linalg.norm(b_h - A.matvec(x_plain)) / np.linalg.norm(b_h))
     solve(head)
     torch.cuda.synchronize(dev)
     xm = x.cpu().numpy()
@@ -304,6 +395,7 @@ def main():
                        "plain_fp64_ms": round(plain_v, 3), "plain_fp64_iters": pl_[1].iters,
                        "plain_fp64_build_ms": round(pl_[0].ms, 3), "plain_rel_res": relres_plain,
                        "speedup_vs_plain_fp64": round(plain_v / ms, 3),
+                       "forms": forms,
                        "ms_steps": [round(v, 3) for v in ms_head]},
             "e2e": {"value": round(e2e_v, 3), "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,

@@ -31,6 +31,7 @@ struct BState {                   // per (system, rhs) pair, length S * R
   double* thr;
   double* bnorm;
   int* active;                    // 1 while iterating
+  int* sys_live;                  // per system: pairs still iterating
   int* conv_it;                   // iteration counter when it stopped
   int* status;                    // dcu_solve_status
 };
@@ -156,24 +157,10 @@ __device__ __forceinline__ bool system_reduce(double (&v)[ND][R], double* __rest
 
 __device__ __forceinline__ bool g_finished(const BGlobal* g) { return *(volatile const int*)&g->done != 0; }
 
-// After a system's last tile updated its scalars: the last system overall
-// advances the shared counter and decides whether the batch is done.
-__device__ __forceinline__ void system_finished_step(BGlobal* g, int nsys, bool advance) {
-  __threadfence();
-  const int k = atomicAdd(&g->systems_done, 1);
-  if (k == nsys - 1) {
-    g->systems_done = 0;
-    if (advance) {
-      g->pidx ^= 1;
-      if (g->active_count <= 0) {
-        g->done = 1;
-      } else {
-        g->it += 1;
-        if (g->it >= g->maxiter) g->done = 1;
-      }
-    }
-  }
-}
+// A system whose every pair stopped is skipped by all its tiles (nothing reads
+// its vectors or partials any more).
+template <int R>
+__device__ __forceinline__ bool system_idle(const BArgs<R>& a, int sys) { return a.st.sys_live[sys] == 0; }
 
 template <int R>
 __global__ void __launch_bounds__(BT) kb_init(BArgs<R> a, double tol, int tol_mode) {
@@ -219,7 +206,7 @@ __global__ void __launch_bounds__(BT) kb_init(BArgs<R> a, double tol, int tol_mo
       live += run ? 1 : 0;
     }
     atomicAdd(&a.g->active_count, live);
-    system_finished_step(a.g, a.nsys, false);
+    a.st.sys_live[sys] = live;
   }
 }
 
@@ -228,6 +215,7 @@ template <int R>
 __global__ void __launch_bounds__(BT) kb_py(BArgs<R> a) {
   if (g_finished(a.g)) return;
   const int tile = blockIdx.x, sys = a.tile_sys[tile];
+  if (system_idle(a, sys)) return;
   const int row = a.tile_row0[tile] + threadIdx.x;
   if (row >= a.sys_off[sys + 1]) return;
   double beta[R], omega[R];
@@ -262,6 +250,7 @@ template <int R>
 __global__ void __launch_bounds__(BT) kb_ay(BArgs<R> a) {
   if (g_finished(a.g)) return;
   const int tile = blockIdx.x, sys = a.tile_sys[tile];
+  if (system_idle(a, sys)) return;
   const int row = a.tile_row0[tile] + threadIdx.x;
   double v[1][R] = {};
   if (row < a.sys_off[sys + 1]) {
@@ -287,9 +276,9 @@ __global__ void __launch_bounds__(BT) kb_ay(BArgs<R> a) {
         a.st.status[i] = DCU_SOLVE_BREAKDOWN;
         a.st.alpha[i] = a.st.omega[i] = a.st.beta[i] = 0.0;
         atomicSub(&a.g->active_count, 1);
+        a.st.sys_live[sys] -= 1;
       }
     }
-    system_finished_step(a.g, a.nsys, false);
   }
 }
 
@@ -298,6 +287,7 @@ template <int R>
 __global__ void __launch_bounds__(BT) kb_sz(BArgs<R> a) {
   if (g_finished(a.g)) return;
   const int tile = blockIdx.x, sys = a.tile_sys[tile];
+  if (system_idle(a, sys)) return;
   const int row = a.tile_row0[tile] + threadIdx.x;
   if (row >= a.sys_off[sys + 1]) return;
   double nalpha[R];
@@ -325,6 +315,7 @@ template <int R>
 __global__ void __launch_bounds__(BT) kb_az(BArgs<R> a) {
   if (g_finished(a.g)) return;
   const int tile = blockIdx.x, sys = a.tile_sys[tile];
+  if (system_idle(a, sys)) return;
   const int row = a.tile_row0[tile] + threadIdx.x;
   double v[2][R] = {};
   if (row < a.sys_off[sys + 1]) {
@@ -351,9 +342,9 @@ __global__ void __launch_bounds__(BT) kb_az(BArgs<R> a) {
         a.st.status[i] = DCU_SOLVE_BREAKDOWN;
         a.st.alpha[i] = a.st.omega[i] = a.st.beta[i] = 0.0;
         atomicSub(&a.g->active_count, 1);
+        a.st.sys_live[sys] -= 1;
       }
     }
-    system_finished_step(a.g, a.nsys, false);
   }
 }
 
@@ -362,6 +353,7 @@ template <int R>
 __global__ void __launch_bounds__(BT) kb_xr(BArgs<R> a) {
   if (g_finished(a.g)) return;
   const int tile = blockIdx.x, sys = a.tile_sys[tile];
+  if (system_idle(a, sys)) return;
   const int row = a.tile_row0[tile] + threadIdx.x;
   double v[2][R] = {};
   if (row < a.sys_off[sys + 1]) {
@@ -413,9 +405,24 @@ __global__ void __launch_bounds__(BT) kb_xr(BArgs<R> a) {
       if (!a.st.active[i]) {
         a.st.alpha[i] = a.st.omega[i] = a.st.beta[i] = 0.0;
         atomicSub(&a.g->active_count, 1);
+        a.st.sys_live[sys] -= 1;
       }
     }
-    system_finished_step(a.g, a.nsys, true);
+  }
+}
+
+// K6: one thread advances the shared counter after K5 and decides whether the
+// batch is done.
+template <int R>
+__global__ void kb_step(BArgs<R> a) {
+  if (g_finished(a.g)) return;
+  BGlobal* g = a.g;
+  g->pidx ^= 1;
+  if (g->active_count <= 0) {
+    g->done = 1;
+  } else {
+    g->it += 1;
+    if (g->it >= g->maxiter) g->done = 1;
   }
 }
 
@@ -456,7 +463,7 @@ int run_batch(Ctx* c, int nsys, const int* sys_off_d, const SellPlan& plan, cons
   const size_t pairs = (size_t)nsys * R;
   const size_t small = al(sizeof(int) * (2 * (size_t)ntiles + nsys + 1)) + al(sizeof(unsigned) * nsys) +
                        al(sizeof(double) * 3 * R * (size_t)ntiles) + al(sizeof(double) * 7 * pairs) +
-                       al(sizeof(int) * 3 * pairs) + al(sizeof(BGlobal));
+                       al(sizeof(int) * 3 * pairs) + al(sizeof(int) * (size_t)nsys) + al(sizeof(BGlobal));
   DCU_TRY(ensure(c, B_VEC, 9 * vec + small));
   char* p = bp<char>(c, B_VEC);
   BArgs<R> a{};
@@ -491,6 +498,8 @@ int run_batch(Ctx* c, int nsys, const int* sys_off_d, const SellPlan& plan, cons
   int* ist = reinterpret_cast<int*>(q);
   a.st.active = ist; a.st.conv_it = ist + pairs; a.st.status = ist + 2 * pairs;
   q += al(sizeof(int) * 3 * pairs);
+  a.st.sys_live = reinterpret_cast<int*>(q);
+  q += al(sizeof(int) * (size_t)nsys);
   a.g = reinterpret_cast<BGlobal*>(q);
   DCU_CUDA(c, cudaMemcpyAsync(tiles, tsys.data(), sizeof(int) * ntiles, cudaMemcpyHostToDevice, c->stream));
   DCU_CUDA(c, cudaMemcpyAsync(tiles + ntiles, trow.data(), sizeof(int) * ntiles, cudaMemcpyHostToDevice, c->stream));
@@ -520,12 +529,13 @@ int run_batch(Ctx* c, int nsys, const int* sys_off_d, const SellPlan& plan, cons
       kb_sz<R><<<ntiles, BT, 0, c->stream>>>(a);
       kb_az<R><<<ntiles, BT, 0, c->stream>>>(a);
       kb_xr<R><<<ntiles, BT, 0, c->stream>>>(a);
+      kb_step<R><<<1, 1, 0, c->stream>>>(a);
     }
     cudaError_t e = cudaStreamEndCapture(c->stream, &gr);
     if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture", __FILE__, __LINE__);
     GraphSlot ne;
     ne.key = key;
-    ne.nodes = 5 * BCHUNK;
+    ne.nodes = 6 * BCHUNK;
     e = cudaGraphInstantiate(&ne.exec, gr, 0);
     cudaGraphDestroy(gr);
     if (e != cudaSuccess) return cuda_fail(c, e, "cudaGraphInstantiate", __FILE__, __LINE__);
