@@ -50,10 +50,22 @@ def workload(m=128, pe=20.0):
     return A, b, xt
 
 
+def iteration_kernels(w_m):
+    """Names of the iteration kernels in launch order: K1 is split in two
+    (streaming p update + one-vector SpMV) when M is narrower than FP64."""
+    k1 = ["k_bi_p", "k_bi_y"] if w_m < 8 else ["k_bi_py"]
+    return k1 + ["k_bi_ay", "k_bi_sz", "k_bi_az", "k_bi_xr"]
+
+
 def bytes_per_kernel(n, nnz, w_m, w_v, w_i):
-    """Algorithmic HBM bytes of the five fused iteration kernels (one launch)."""
-    return [
-        nnz * (w_m + w_i) + n * (16 + 3 * w_v),   # K1 p = r + beta(p - w ay), y = M p
+    """Algorithmic HBM bytes of each iteration kernel (one launch), in the
+    order of iteration_kernels()."""
+    if w_m < 8:
+        k1 = [n * (16 + 2 * w_v),                           # K1a p = r + beta(p - w ay)
+              nnz * (w_m + w_i) + n * 2 * w_v]              # K1b y = M p
+    else:
+        k1 = [nnz * (w_m + w_i) + n * (16 + 3 * w_v)]      # K1 p on the fly, y = M p
+    return k1 + [
         nnz * (8 + w_i) + n * (8 + 2 * w_v),      # K2 ay = A y, (r*, ay)
         nnz * (w_m + w_i) + n * (24 + w_v),       # K3 s = r - alpha ay, z = M s
         nnz * (8 + w_i) + n * (16 + w_v),         # K4 az = A z, (az, s), (az, az)
@@ -336,7 +348,9 @@ def main():
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = kbytes[j] / (kms[j] * 1e-3) / 1e9
-    roofline = {"bound": "hbm", "kernel": ["k_bi_py", "k_bi_ay", "k_bi_sz", "k_bi_az", "k_bi_xr"][j],
+    names = iteration_kernels(w_m)
+    assert len(names) == len(kms) == len(kbytes), (names, kms)
+    roofline = {"bound": "hbm", "kernel": names[j],
                 "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 3),
                 "traffic": None, "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                 "kernel_ms": [round(v, 4) for v in kms],

@@ -151,9 +151,10 @@ class Context:
         return info
 
     def profile_iteration(self, reps: int = 20):
-        ms = (C.c_float * 5)()
-        self._check(self._L.dcu_profile_iteration_kernels(self.h, reps, ms))
-        return [float(v) for v in ms]
+        ms = (C.c_float * 16)()
+        cnt = C.c_int(0)
+        self._check(self._L.dcu_profile_iteration_kernels(self.h, reps, ms, 16, C.byref(cnt)))
+        return [float(ms[i]) for i in range(cnt.value)]
 
     def csc_to_csr_d(self, n, nnz, ptr_d, idx_d, val_d, rptr_d, ridx_d, rval_d):
         self._check(self._L.dcu_csc_to_csr_d(self.h, n, nnz, _p(ptr_d), _p(idx_d), _p(val_d), _p(rptr_d),

@@ -26,6 +26,7 @@
 #include <cmath>
 #include <algorithm>
 #include <cstddef>
+#include <type_traits>
 
 #include "internal.cuh"
 
@@ -239,6 +240,59 @@ __global__ void __launch_bounds__(BI_BLOCK) k_bi_py(BiArgs<MT, IT, VT> a) {
   }
 }
 
+// Split form of K1, used with a narrow (FP32 / BF16) preconditioner: p is
+// formed once per row by a streaming kernel and then read by a one-vector
+// SpMV, instead of at every gathered column (three gathered vectors per
+// entry).  Same arithmetic as the fused kernel.  With an FP64 M the SpMV
+// itself moves 8 bytes of value per entry and the extra launch and pass cost
+// more than the gathers they save, so K1 stays fused there; K3 gathers two
+// vectors and stays fused always.
+template <typename MT>
+constexpr bool split_k1() {
+  return !std::is_same<MT, double>::value;
+}
+
+__device__ __forceinline__ double2 ld2(const double* p) { return *reinterpret_cast<const double2*>(p); }
+__device__ __forceinline__ double2 ld2(const float* p) {
+  const float2 f = *reinterpret_cast<const float2*>(p);
+  return make_double2((double)f.x, (double)f.y);
+}
+__device__ __forceinline__ void st2(double* p, double u, double v) {
+  *reinterpret_cast<double2*>(p) = make_double2(u, v);
+}
+__device__ __forceinline__ void st2(float* p, double u, double v) {
+  *reinterpret_cast<float2*>(p) = make_float2((float)u, (float)v);
+}
+
+// K1a: p = r + beta (p - omega ay), in place (p0)
+template <typename MT, typename IT, typename VT>
+__global__ void __launch_bounds__(BI_BLOCK) k_bi_p(BiArgs<MT, IT, VT> a) {
+  if (finished(a.S)) return;
+  const double beta = a.S->beta, omega = a.S->omega;
+  auto pf = [&](double rv, double pv, double ayv) { return rv + beta * (pv - omega * ayv); };
+  const int npair = a.n >> 1;
+  const int stride = gridDim.x * BI_BLOCK;
+  for (int q = blockIdx.x * BI_BLOCK + threadIdx.x; q < npair; q += stride) {
+    const int r = 2 * q;
+    const double2 r2 = ld2(a.r + r), p2 = ld2(a.p0 + r), y2 = ld2(a.ay + r);
+    st2(a.p0 + r, pf(r2.x, p2.x, y2.x), pf(r2.y, p2.y, y2.y));
+  }
+  if ((a.n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+    const int r = a.n - 1;
+    a.p0[r] = (VT)pf(a.r[r], (double)a.p0[r], a.ay[r]);
+  }
+}
+
+// K1b: y = M p
+template <typename MT, typename IT, typename VT>
+__global__ void __launch_bounds__(BI_BLOCK) k_bi_y(BiArgs<MT, IT, VT> a) {
+  if (finished(a.S)) return;
+  const VT* __restrict__ p = a.p0;
+  const int stride = gridDim.x * BI_BLOCK;
+  for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride)
+    a.y[r] = (VT)sell_row(a.off, a.mval, a.ix, r, [&](int c) { return ldv(p + c); });
+}
+
 // K2: ay = A y; alpha = rho / (r*, ay)
 template <typename MT, typename IT, typename VT>
 __global__ void __launch_bounds__(BI_BLOCK) k_bi_ay(BiArgs<MT, IT, VT> a) {
@@ -304,22 +358,43 @@ __global__ void __launch_bounds__(BI_BLOCK) k_bi_az(BiArgs<MT, IT, VT> a) {
   }
 }
 
-// K5: x += alpha y + omega z; r = s - omega az; rho, beta, ||r||, stop test
+// K5: x += alpha y + omega z; r = s - omega az; rho, beta, ||r||, stop test.
+// Rows are taken in pairs with every load issued before the first store
+// (16-byte loads of the FP64 vectors), so one DRAM round trip covers a pair.
 template <typename MT, typename IT, typename VT>
-__global__ void __launch_bounds__(BI_BLOCK) k_bi_xr(BiArgs<MT, IT, VT> a) {
+__global__ void __launch_bounds__(BI_BLOCK, 6) k_bi_xr(BiArgs<MT, IT, VT> a) {
   if (finished(a.S)) return;
   const double alpha = a.S->alpha, omega = a.S->omega, nomega = -1.0 * omega;
   double v[2] = {0.0, 0.0};
-  const int stride = gridDim.x * BI_BLOCK;
-  for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) {
-    double xv = a.x[r];
-    xv = xv + alpha * (double)a.y[r];
-    xv = xv + omega * (double)a.z[r];
-    a.x[r] = xv;
-    const double rn = a.s[r] + nomega * a.az[r];
-    a.r[r] = rn;
-    v[0] += (double)a.rs[r] * rn;
+  auto row = [&](double& xv, double yv, double zv, double sv, double azv, double rsv) {
+    xv = xv + alpha * yv;
+    xv = xv + omega * zv;
+    const double rn = sv + nomega * azv;
+    v[0] += rsv * rn;
     v[1] += rn * rn;
+    return rn;
+  };
+  const int npair = a.n >> 1;
+  const int stride = gridDim.x * BI_BLOCK;
+  for (int q = blockIdx.x * BI_BLOCK + threadIdx.x; q < npair; q += stride) {
+    const int r = 2 * q;
+    double2 x2 = *reinterpret_cast<const double2*>(a.x + r);
+    const double2 s2 = *reinterpret_cast<const double2*>(a.s + r);
+    const double2 az2 = *reinterpret_cast<const double2*>(a.az + r);
+    const double y0 = (double)a.y[r], y1 = (double)a.y[r + 1];
+    const double z0 = (double)a.z[r], z1 = (double)a.z[r + 1];
+    const double rs0 = (double)a.rs[r], rs1 = (double)a.rs[r + 1];
+    const double r0 = row(x2.x, y0, z0, s2.x, az2.x, rs0);
+    const double r1 = row(x2.y, y1, z1, s2.y, az2.y, rs1);
+    *reinterpret_cast<double2*>(a.x + r) = x2;
+    *reinterpret_cast<double2*>(a.r + r) = make_double2(r0, r1);
+  }
+  if ((a.n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+    const int r = a.n - 1;
+    double xv = a.x[r];
+    const double rn = row(xv, (double)a.y[r], (double)a.z[r], a.s[r], a.az[r], (double)a.rs[r]);
+    a.x[r] = xv;
+    a.r[r] = rn;
   }
   double tot[2];
   if (grid_reduce<2>(v, a.part, &a.S->counter[3], tot) && threadIdx.x == 0) {
@@ -421,7 +496,10 @@ int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval,
   const int g_az = gsize((const void*)k_bi_az<MT, IT, VT>);
   const int g_xr = gsize((const void*)k_bi_xr<MT, IT, VT>);
   const int g_tr = gsize((const void*)k_bi_true<MT, IT, VT>);
-  const int grid = std::max({g_init, g_py, g_ay, g_sz, g_az, g_xr, g_tr});  // partial-sum slots
+  const int g_p = gsize((const void*)k_bi_p<MT, IT, VT>);
+  const int g_y = gsize((const void*)k_bi_y<MT, IT, VT>);
+  const int grid = std::max({g_init, g_py, g_ay, g_sz, g_az, g_xr, g_tr, g_p, g_y});
+  constexpr bool split = split_k1<MT>();  // partial-sum slots
   // vectors: r, ay, s, az (double) + rs, p0, p1, y, z (VT), 256-byte aligned
   auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
   const size_t nd = al(sizeof(double) * (size_t)n), nv = al(sizeof(VT) * (size_t)n);
@@ -448,6 +526,8 @@ int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval,
   a.z = (VT*)(base + 4 * nd + 4 * nv);
   a.part = bp<double>(c, B_PART);
   a.S = bp<Scal>(c, B_SCAL);
+  if (reinterpret_cast<uintptr_t>(x) % 16 != 0)
+    return fail(c, DCU_ERR_ARG, "x must be 16-byte aligned (cudaMalloc pointers are)");
   DCU_CUDA(c, cudaMemsetAsync(a.S, 0, sizeof(Scal), c->stream));
   int maxiter = opt->maxiter > 0 ? opt->maxiter : n;  // bicgstab_solver.h:134
   DCU_CUDA(c, cudaEventRecord(c->ev[0], c->stream));
@@ -467,7 +547,12 @@ int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval,
     DCU_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     cudaError_t le = cudaSuccess;
     for (int i = 0; i < CHUNK_ITERS && le == cudaSuccess; ++i) {
-      le = launch_pdl(k_bi_py<MT, IT, VT>, g_py, c->stream, a);
+      if (split) {
+        le = launch_pdl(k_bi_p<MT, IT, VT>, g_p, c->stream, a);
+        if (le == cudaSuccess) le = launch_pdl(k_bi_y<MT, IT, VT>, g_y, c->stream, a);
+      } else {
+        le = launch_pdl(k_bi_py<MT, IT, VT>, g_py, c->stream, a);
+      }
       if (le == cudaSuccess) le = launch_pdl(k_bi_ay<MT, IT, VT>, g_ay, c->stream, a);
       if (le == cudaSuccess) le = launch_pdl(k_bi_sz<MT, IT, VT>, g_sz, c->stream, a);
       if (le == cudaSuccess) le = launch_pdl(k_bi_az<MT, IT, VT>, g_az, c->stream, a);
@@ -481,7 +566,7 @@ int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval,
     if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture", __FILE__, __LINE__);
     GraphSlot ne;
     ne.key = key;
-    ne.nodes = 5 * CHUNK_ITERS;
+    ne.nodes = (split ? 6 : 5) * CHUNK_ITERS;
     e = cudaGraphInstantiate(&ne.exec, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return cuda_fail(c, e, "cudaGraphInstantiate", __FILE__, __LINE__);
@@ -496,15 +581,21 @@ int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval,
   // Chunks are launched one ahead of the flag that is read back, so the GPU
   // never idles on the host; after convergence at most one chunk of
   // early-exit kernels runs.
-  c->profile_kernels = 5;
-  c->profile_launch = [c, a, g_py, g_ay, g_sz, g_az, g_xr](int j) -> int {
+  c->profile_kernels = split ? 6 : 5;
+  c->profile_launch = [c, a, g_py, g_ay, g_sz, g_az, g_xr, g_p, g_y](int j) -> int {
     DCU_CUDA(c, cudaMemsetAsync(&a.S->done, 0, sizeof(int), c->stream));
-    switch (j) {
-      case 0: k_bi_py<MT, IT, VT><<<g_py, BI_BLOCK, 0, c->stream>>>(a); break;
-      case 1: k_bi_ay<MT, IT, VT><<<g_ay, BI_BLOCK, 0, c->stream>>>(a); break;
-      case 2: k_bi_sz<MT, IT, VT><<<g_sz, BI_BLOCK, 0, c->stream>>>(a); break;
-      case 3: k_bi_az<MT, IT, VT><<<g_az, BI_BLOCK, 0, c->stream>>>(a); break;
-      default: k_bi_xr<MT, IT, VT><<<g_xr, BI_BLOCK, 0, c->stream>>>(a); break;
+    if (split && j == 0) {
+      k_bi_p<MT, IT, VT><<<g_p, BI_BLOCK, 0, c->stream>>>(a);
+    } else if (split && j == 1) {
+      k_bi_y<MT, IT, VT><<<g_y, BI_BLOCK, 0, c->stream>>>(a);
+    } else {
+      switch (split ? j - 1 : j) {
+        case 0: k_bi_py<MT, IT, VT><<<g_py, BI_BLOCK, 0, c->stream>>>(a); break;
+        case 1: k_bi_ay<MT, IT, VT><<<g_ay, BI_BLOCK, 0, c->stream>>>(a); break;
+        case 2: k_bi_sz<MT, IT, VT><<<g_sz, BI_BLOCK, 0, c->stream>>>(a); break;
+        case 3: k_bi_az<MT, IT, VT><<<g_az, BI_BLOCK, 0, c->stream>>>(a); break;
+        default: k_bi_xr<MT, IT, VT><<<g_xr, BI_BLOCK, 0, c->stream>>>(a); break;
+      }
     }
     DCU_LAUNCHED(c, "profile kernel");
     return DCU_OK;
@@ -588,8 +679,10 @@ int bicgstab_solve(Ctx* c, const SellPlan& plan, const double* aval_sell, const 
              : run_solver<__nv_bfloat16, int, double>(c, plan, aval_sell, mb, plan.idx, b, x, opt, info);
 }
 
-int profile_iteration(Ctx* c, int reps, float* ms) {
+int profile_iteration(Ctx* c, int reps, float* ms, int cap, int* count) {
   if (!c->profile_launch) return fail(c, DCU_ERR_ARG, "no solve has run on this context");
+  if (count) *count = c->profile_kernels;
+  if (cap < c->profile_kernels) return fail(c, DCU_ERR_ARG, "ms_out holds fewer entries than kernels");
   if (reps < 1) reps = 1;
   // cost of the stop-flag reset that precedes every launch
   int* done = reinterpret_cast<int*>(c->buf[B_SCAL].p) + offsetof(Scal, done) / sizeof(int);

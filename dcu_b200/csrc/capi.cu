@@ -458,10 +458,10 @@ int dcu_batch_solve_d(dcu_spai_ctx* c, int nsys, const int* sys_off, int n, int 
   }
 }
 
-int dcu_profile_iteration_kernels(dcu_spai_ctx* c, int reps, float* ms_out) {
+int dcu_profile_iteration_kernels(dcu_spai_ctx* c, int reps, float* ms_out, int cap, int* count) {
   if (!c || !ms_out) return DCU_ERR_ARG;
   StreamScope scope(c);
-  return dcu::profile_iteration(c, reps, ms_out);
+  return dcu::profile_iteration(c, reps, ms_out, cap, count);
 }
 
 int dcu_spai_solve_h(dcu_spai_ctx* c, int n, int nnz, const int* ptr, const int* idx, const double* val,

@@ -171,7 +171,7 @@ int check_blocks(Ctx* c, int n, const int* ptr, const int* idx, int nsys, const 
 int batch_solve(Ctx* c, int nsys, const int* sys_off, const SellPlan& plan, const double* aval, const double* mval,
                 int nrhs, const double* B, double* X, const dcu_options* opt, int* iters, int* status,
                 dcu_solve_info* info);
-int profile_iteration(Ctx* c, int reps, float* ms);
+int profile_iteration(Ctx* c, int reps, float* ms, int cap, int* count);
 
 // grid size for grid-stride kernels: whole waves of `per_sm` blocks
 inline int waves_grid(const Ctx* c, long long work_items, int block, int per_sm) {

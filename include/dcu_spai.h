@@ -27,7 +27,9 @@
  * (int32), val[nnz] (float64) -- the CSC_Matrix layout of
  * include/common/dataType.h:33-41.  The preconditioner M has A's pattern, so
  * it is passed as values only (mval[nnz], aligned with A's idx).
- * Suffix _d: device pointers (cudaMalloc'ed, on the context's device);
+ * Suffix _d: device pointers (cudaMalloc'ed, on the context's device; the
+ * solution vector x must be 16-byte aligned, as cudaMalloc and torch
+ * allocations are, else DCU_ERR_ARG);
  * suffix _h: host pointers (copies are made inside the call).
  */
 #ifndef DCU_SPAI_H
@@ -256,12 +258,16 @@ int dcu_batch_solve_d(dcu_spai_ctx* ctx, int nsys, const int* sys_off, int n, in
                       const dcu_options* opt, double* mval, int* iters, int* status,
                       dcu_build_info* binfo, dcu_solve_info* sinfo);
 
-/* Diagnostic timing: re-launch each of the five fused iteration kernels of
- * the last solve on this context (K1 p/y = M p, K2 A y + (r*,Ay), K3 s/z = M s,
- * K4 A z + dots, K5 x/r update + dots) `reps` times on that solve's buffers
- * and write the mean device time per launch (ms) to ms_out[0..4].  The
- * solver vectors and x are left in an unspecified state. */
-int dcu_profile_iteration_kernels(dcu_spai_ctx* ctx, int reps, float* ms_out);
+/* Diagnostic timing: re-launch each iteration kernel of the last solve on
+ * this context `reps` times on that solve's buffers and write the mean device
+ * time per launch (ms) to ms_out[0..count-1], in launch order.  With an FP64
+ * preconditioner the iteration runs five fused kernels:
+ *   p/y = M p | A y + (r*, Ay) | s/z = M s | A z + dots | x/r update + dots
+ * with a narrow (FP32 / BF16) preconditioner six, the first one split in two:
+ *   p = r + beta (p - omega Ay) | y = M p | ... (as above)
+ * *count (optional) receives the number of kernels; DCU_ERR_ARG when cap is
+ * smaller.  The solver vectors and x are left in an unspecified state. */
+int dcu_profile_iteration_kernels(dcu_spai_ctx* ctx, int reps, float* ms_out, int cap, int* count);
 
 /* ---- MatrixMarket input (command-line driver) --------------------------------- */
 
