@@ -283,9 +283,9 @@ __global__ void __launch_bounds__(BI_BLOCK) k_bi_p(BiArgs<MT, IT, VT> a) {
   }
 }
 
-// K1b: y = M p
+// K1b: y = M p (held to 32 registers: 8 blocks per SM; at 34 it ran 6)
 template <typename MT, typename IT, typename VT>
-__global__ void __launch_bounds__(BI_BLOCK) k_bi_y(BiArgs<MT, IT, VT> a) {
+__global__ void __launch_bounds__(BI_BLOCK, 8) k_bi_y(BiArgs<MT, IT, VT> a) {
   if (finished(a.S)) return;
   const VT* __restrict__ p = a.p0;
   const int stride = gridDim.x * BI_BLOCK;

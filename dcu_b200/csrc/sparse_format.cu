@@ -36,6 +36,46 @@ __global__ void k_row_scatter(const int* __restrict__ ptr, const int* __restrict
   }
 }
 
+// Structurally symmetric patterns (every PDE stencil): row c of A lists the
+// same indices as column c, so with ascending row indices in every column the
+// CSR index arrays are the CSC ones, and only the CSR slot -> CSC slot map
+// needs work: entry (row c, column r) sits in column r where idx == c, found
+// by binary search.  One thread per column; flag bit 1 = a column is not
+// strictly ascending, bit 2 = some (r, c) has no (c, r).  Any flag sends the
+// conversion to the general count / scatter / sort path, which rewrites all
+// three outputs.
+__global__ void k_csr_symmetric(const int* __restrict__ ptr, const int* __restrict__ idx, int n,
+                                int* __restrict__ rptr, int* __restrict__ rcol, int* __restrict__ rperm,
+                                int* __restrict__ flag) {
+  int bad = 0;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+    const int s = ptr[c], e = ptr[c + 1];
+    rptr[c] = s;
+    if (c == n - 1) rptr[n] = e;
+    int prev = -1;
+    for (int k = s; k < e; ++k) {
+      const int r = idx[k];
+      rcol[k] = r;
+      if (r <= prev) bad |= 1;
+      prev = r;
+      int lo = ptr[r], hi = ptr[r + 1] - 1, q = -1;
+      while (lo <= hi) {
+        const int mid = (lo + hi) >> 1;
+        const int v = idx[mid];
+        if (v == c) {
+          q = mid;
+          break;
+        }
+        if (v < c) lo = mid + 1;
+        else hi = mid - 1;
+      }
+      if (q < 0) bad |= 2;
+      rperm[k] = q;
+    }
+  }
+  if (__any_sync(0xffffffffu, bad != 0) && bad) atomicOr(flag, bad);
+}
+
 constexpr int kRegSortMax = 16;     // rows sorted in registers by one thread
 constexpr int kThreadSortMax = 64;  // rows sorted in place by one thread
 
@@ -317,8 +357,16 @@ int csr_from_csc(Ctx* c, int n, int nnz, const int* ptr, const int* idx, int* rp
   int* cnt = bp<int>(c, B_ROWCNT);
   int* longrows = bp<int>(c, B_LONGROWS);
   int* longcount = longrows + n;  // [0] = count, [1] = longest length
-  DCU_CUDA(c, cudaMemsetAsync(cnt, 0, sizeof(int) * (size_t)(n + 1), c->stream));
   DCU_CUDA(c, cudaMemsetAsync(longcount, 0, 2 * sizeof(int), c->stream));
+  if (n > 0 && nnz > 0) {
+    k_csr_symmetric<<<waves_grid(c, n, 256, 8), 256, 0, c->stream>>>(ptr, idx, n, rptr, rcol, rperm, longcount);
+    DCU_LAUNCHED(c, "k_csr_symmetric");
+    DCU_CUDA(c, cudaMemcpyAsync(c->pinned, longcount, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    DCU_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (*(int*)c->pinned == 0) return DCU_OK;
+    DCU_CUDA(c, cudaMemsetAsync(longcount, 0, 2 * sizeof(int), c->stream));
+  }
+  DCU_CUDA(c, cudaMemsetAsync(cnt, 0, sizeof(int) * (size_t)(n + 1), c->stream));
   if (nnz > 0) {
     k_row_count<<<waves_grid(c, nnz, 256, 8), 256, 0, c->stream>>>(idx, nnz, cnt);
     DCU_LAUNCHED(c, "k_row_count");

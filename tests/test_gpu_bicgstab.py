@@ -76,10 +76,54 @@ def test_maxiter_counter(ctx):
     assert info.iters == 5   # the reference's counter runs 1..MAX_ITER
 
 
-def test_csr_matches_oracle(ctx):
+def _shuffled_columns(A, seed):
+    """Same matrix with each column's entries in a seeded random order."""
+    rng = np.random.default_rng(seed)
+    idx, val = A.idx.copy(), A.val.copy()
+    for c in range(A.n):
+        s, e = A.ptr[c], A.ptr[c + 1]
+        o = rng.permutation(e - s)
+        idx[s:e], val[s:e] = idx[s:e][o], val[s:e][o]
+    return W.CSC(A.n, A.ptr, idx, val)
+
+
+def _one_sided(A):
+    """A's pattern with one off-diagonal entry removed: no longer symmetric."""
+    c = A.n // 2
+    s, e = A.ptr[c], A.ptr[c + 1]
+    drop = next(k for k in range(s, e) if A.idx[k] != c)
+    keep = np.ones(A.nnz, bool)
+    keep[drop] = False
+    ptr = A.ptr.copy()
+    ptr[c + 1:] -= 1
+    return W.CSC(A.n, ptr, A.idx[keep], A.val[keep])
+
+
+def _empty_columns(A):
+    """Symmetric pattern with a whole row/column pair (index 5) emptied."""
+    keep = np.ones(A.nnz, bool)
+    cols = np.repeat(np.arange(A.n), np.diff(A.ptr))
+    keep[(A.idx == 5) | (cols == 5)] = False
+    ptr = np.zeros(A.n + 1, np.int32)
+    ptr[1:] = np.cumsum(np.bincount(cols[keep], minlength=A.n))
+    return W.CSC(A.n, ptr, A.idx[keep], A.val[keep])
+
+
+CSR_CASES = {
+    "circuit": lambda: W.circuit_like(),                              # general path
+    "cd2d_64": lambda: W.convdiff2d(64, 10.0),                        # symmetric pattern
+    "cd3d_16": lambda: W.convdiff3d(16, 20.0),                        # symmetric pattern
+    "cd2d_shuffled": lambda: _shuffled_columns(W.convdiff2d(32, 10.0), 3),  # symmetric, unsorted
+    "cd2d_one_sided": lambda: _one_sided(W.convdiff2d(32, 10.0)),     # almost symmetric
+    "cd2d_empty": lambda: _empty_columns(W.convdiff2d(32, 10.0)),     # symmetric, empty column
+}
+
+
+@pytest.mark.parametrize("case", list(CSR_CASES))
+def test_csr_matches_oracle(ctx, case):
     import torch
 
-    A = W.circuit_like()
+    A = CSR_CASES[case]()
     rp_o, ri_o, rv_o = oracle.csc2csr(A.n, A.ptr, A.idx, A.val)
     d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
     rp = torch.zeros(A.n + 1, dtype=torch.int32, device="cuda")
