@@ -83,6 +83,36 @@ int prepare_solve(Ctx* c, int n, int nnz, const int* ptr, const int* idx, const 
   return gather_values(c, *plan, val, mval, precision, msell);
 }
 
+// The whole path on device arrays: validation, the SELL plan (pattern only),
+// the SPAI build, A and M in SELL order, BiCGSTAB.  When the values or the
+// vectors are still being copied in on the copy stream, val_ready / bx_ready
+// (optional) are the events that mark their arrival: the plan is built while
+// the values are in flight, and the build while b and x0 are.
+int solve_pipeline(Ctx* c, int n, int nnz, const int* ptr, const int* idx, const double* val, const double* b,
+                   double* x, const dcu_options& o, double* mval, dcu_build_info* binfo, dcu_solve_info* sinfo,
+                   cudaEvent_t val_ready, cudaEvent_t bx_ready) {
+  double* m = mval;
+  if (!m) {
+    DCU_TRY(dcu::ensure(c, dcu::B_MVAL, sizeof(double) * (size_t)(nnz > 0 ? nnz : 1)));
+    m = dcu::bp<double>(c, dcu::B_MVAL);
+  }
+  DCU_TRY(dcu::validate_csc(c, n, nnz, ptr, idx));
+  dcu::SellPlan plan;
+  DCU_TRY(dcu::sell_plan(c, n, nnz, ptr, idx, &plan));
+  if (val_ready) DCU_CUDA(c, cudaStreamWaitEvent(c->stream, val_ready, 0));
+  dcu_build_info bl{};
+  DCU_CUDA(c, cudaEventRecord(c->ev[0], c->stream));
+  DCU_TRY(dcu::spai_build(c, n, nnz, ptr, idx, val, &o, m, nullptr, &bl));
+  DCU_CUDA(c, cudaEventRecord(c->ev[1], c->stream));
+  DCU_CUDA(c, cudaEventSynchronize(c->ev[1]));
+  cudaEventElapsedTime(&bl.ms, c->ev[0], c->ev[1]);
+  if (binfo) *binfo = bl;
+  const void* msell = nullptr;
+  DCU_TRY(gather_values(c, plan, val, m, o.precision, &msell));
+  if (bx_ready) DCU_CUDA(c, cudaStreamWaitEvent(c->stream, bx_ready, 0));
+  return dcu::bicgstab_solve(c, plan, dcu::bp<double>(c, dcu::B_SELL_AVAL), msell, b, x, &o, sinfo);
+}
+
 // Host uploads share one buffer: ptr | idx | val | b | x | mval.
 struct Uploads {
   int* ptr;
@@ -155,6 +185,7 @@ int dcu_spai_create(dcu_spai_ctx** out, int device, int units) {
     c->max_threads_sm = prop.maxThreadsPerMultiProcessor;
     c->smem_optin = prop.sharedMemPerBlockOptin;
     if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) { rc = dcu::cuda_fail(c, e, "stream", __FILE__, __LINE__); break; }
+    if ((e = cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking)) != cudaSuccess) { rc = dcu::cuda_fail(c, e, "copy stream", __FILE__, __LINE__); break; }
     if ((e = cudaMallocHost(&c->pinned, dcu::kPinnedBytes)) != cudaSuccess) { rc = dcu::cuda_fail(c, e, "cudaMallocHost", __FILE__, __LINE__); break; }
     for (int i = 0; i < 4 && e == cudaSuccess; ++i)
       e = cudaEventCreateWithFlags(&c->ev[i], i < 2 ? cudaEventDefault : cudaEventDisableTiming);
@@ -177,6 +208,7 @@ void dcu_spai_destroy(dcu_spai_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
   dcu::release_graphs(c);
   for (auto& b : c->buf)
     if (b.p) cudaFree(b.p);
@@ -185,6 +217,7 @@ void dcu_spai_destroy(dcu_spai_ctx* c) {
   if (c->ev_sync) cudaEventDestroy(c->ev_sync);
   if (c->pinned) cudaFreeHost(c->pinned);
   if (c->stream) cudaStreamDestroy(c->stream);
+  if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
   delete c;
 }
 
@@ -364,23 +397,7 @@ int dcu_spai_solve_d(dcu_spai_ctx* c, int n, int nnz, const int* ptr, const int*
   if ((rc = resolve_range(c, n, opt, &o))) return rc;
   try {
     StreamScope scope(c);
-    double* m = mval;
-    if (!m) {
-      DCU_TRY(dcu::ensure(c, dcu::B_MVAL, sizeof(double) * (size_t)(nnz > 0 ? nnz : 1)));
-      m = dcu::bp<double>(c, dcu::B_MVAL);
-    }
-    dcu_build_info bl{};
-    DCU_TRY(dcu::validate_csc(c, n, nnz, ptr, idx));
-    DCU_CUDA(c, cudaEventRecord(c->ev[0], c->stream));
-    DCU_TRY(dcu::spai_build(c, n, nnz, ptr, idx, val, &o, m, nullptr, &bl));
-    DCU_CUDA(c, cudaEventRecord(c->ev[1], c->stream));
-    DCU_CUDA(c, cudaEventSynchronize(c->ev[1]));
-    cudaEventElapsedTime(&bl.ms, c->ev[0], c->ev[1]);
-    if (binfo) *binfo = bl;
-    dcu::SellPlan plan;
-    const void* msell = nullptr;
-    DCU_TRY(prepare_solve(c, n, nnz, ptr, idx, val, m, o.precision, &plan, &msell));
-    return dcu::bicgstab_solve(c, plan, dcu::bp<double>(c, dcu::B_SELL_AVAL), msell, b, x, &o, sinfo);
+    return solve_pipeline(c, n, nnz, ptr, idx, val, b, x, o, mval, binfo, sinfo, nullptr, nullptr);
   } catch (const std::bad_alloc&) {
     return dcu::fail(c, DCU_ERR_ALLOC, "host allocation failed");
   }
@@ -470,10 +487,43 @@ int dcu_spai_solve_h(dcu_spai_ctx* c, int n, int nnz, const int* ptr, const int*
   int rc = check_matrix(c, n, nnz, ptr, idx, val);
   if (rc) return rc;
   if (!b || !x) return dcu::fail(c, DCU_ERR_ARG, "null vector");
+  dcu_options o;
+  if ((rc = resolve_range(c, n, opt, &o))) return rc;
   StreamScope scope(c);
-  Uploads u;
-  DCU_TRY(upload(c, n, nnz, ptr, idx, val, b, x, true, &u));
-  rc = dcu_spai_solve_d(c, n, nnz, u.ptr, u.idx, u.val, u.b, u.x, opt, u.mval, binfo, sinfo);
+  // ptr and idx first on the context stream (the analysis needs only them);
+  // values, then b and x0, on the copy stream while the analysis and the
+  // build run.  With pinned host buffers the copies overlap that work.
+  auto al = [](size_t v) { return (v + 255) & ~(size_t)255; };
+  const size_t sp = al(sizeof(int) * (size_t)(n + 1)), si = al(sizeof(int) * (size_t)(nnz > 0 ? nnz : 1));
+  const size_t sv = al(sizeof(double) * (size_t)(nnz > 0 ? nnz : 1)), sn = al(sizeof(double) * (size_t)n);
+  DCU_TRY(dcu::ensure(c, dcu::B_UPLOAD, sp + si + 2 * sv + 2 * sn));
+  char* base = dcu::bp<char>(c, dcu::B_UPLOAD);
+  Uploads u{(int*)base, (int*)(base + sp), (double*)(base + sp + si), (double*)(base + sp + si + sv),
+            (double*)(base + sp + si + sv + sn), (double*)(base + sp + si + sv + 2 * sn)};
+  // On every return, including early ones, no copy may still be reading the
+  // caller's host buffers.
+  struct CopyDrain {
+    Ctx* c;
+    ~CopyDrain() { cudaStreamSynchronize(c->copy_stream); }
+  } drain{c};
+  // the copy stream starts after everything already queued on the context
+  // stream (earlier users of the upload buffer)
+  DCU_CUDA(c, cudaEventRecord(c->ev[2], c->stream));
+  DCU_CUDA(c, cudaStreamWaitEvent(c->copy_stream, c->ev[2], 0));
+  DCU_CUDA(c, cudaMemcpyAsync(u.ptr, ptr, sizeof(int) * (size_t)(n + 1), cudaMemcpyHostToDevice, c->stream));
+  if (nnz > 0) {
+    DCU_CUDA(c, cudaMemcpyAsync(u.idx, idx, sizeof(int) * (size_t)nnz, cudaMemcpyHostToDevice, c->stream));
+    DCU_CUDA(c, cudaMemcpyAsync(u.val, val, sizeof(double) * (size_t)nnz, cudaMemcpyHostToDevice, c->copy_stream));
+  }
+  DCU_CUDA(c, cudaEventRecord(c->ev[2], c->copy_stream));
+  DCU_CUDA(c, cudaMemcpyAsync(u.b, b, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, c->copy_stream));
+  DCU_CUDA(c, cudaMemcpyAsync(u.x, x, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, c->copy_stream));
+  DCU_CUDA(c, cudaEventRecord(c->ev[3], c->copy_stream));
+  try {
+    rc = solve_pipeline(c, n, nnz, u.ptr, u.idx, u.val, u.b, u.x, o, u.mval, binfo, sinfo, c->ev[2], c->ev[3]);
+  } catch (const std::bad_alloc&) {
+    rc = dcu::fail(c, DCU_ERR_ALLOC, "host allocation failed");
+  }
   if (rc) return rc;
   DCU_CUDA(c, cudaMemcpyAsync(x, u.x, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
   if (mval && nnz > 0)

@@ -133,3 +133,28 @@ def test_csr_matches_oracle(ctx, case):
     assert np.array_equal(rp.cpu().numpy(), rp_o)
     assert np.array_equal(ri.cpu().numpy(), ri_o)
     assert np.array_equal(rv.cpu().numpy(), rv_o)
+
+
+def test_host_path_matches_device_path(ctx):
+    """dcu_spai_solve_h (uploads overlapped with the analysis and the build)
+    returns exactly what dcu_spai_solve_d returns, from pageable and from
+    pinned host buffers, with a nonzero x0."""
+    import torch
+
+    A = W.convdiff3d(24, 20.0)
+    b, _ = W.rhs_from_solution(A, seed=4)
+    x0 = np.random.default_rng(9).standard_normal(A.n) * 1e-3
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    xd = d(x0)
+    md = torch.zeros(A.nnz, dtype=torch.float64, device="cuda")
+    ctx.solve_d(A.n, A.nnz, d(A.ptr), d(A.idx), d(A.val), d(b), xd, mval_d=md, precision=N.PREC_M_BF16)
+    x_dev, m_dev = xd.cpu().numpy(), md.cpu().numpy()
+
+    x_h, m_h, _, si = ctx.solve_h(A, b, x0=x0, want_m=True, precision=N.PREC_M_BF16)
+    assert si.status == N.SOLVE_CONVERGED
+    assert np.array_equal(x_h, x_dev) and np.array_equal(m_h, m_dev)
+
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+    hx, hm = pin(x0), pin(np.zeros(A.nnz))
+    ctx.solve_h_into(A.n, A.nnz, pin(A.ptr), pin(A.idx), pin(A.val), pin(b), hx, mval=hm, precision=N.PREC_M_BF16)
+    assert np.array_equal(hx, x_dev) and np.array_equal(hm, m_dev)
