@@ -73,6 +73,16 @@ def bytes_per_kernel(n, nnz, w_m, w_v, w_i):
     ]
 
 
+# DRAM bytes (read + write) of one launch of each iteration kernel at 128^3,
+# from one ncu capture per kernel (profiles/iteration_kernels_128cube.md;
+# cold L2, single launch), keyed by (kernel, form).
+TRAFFIC_BYTES = {
+    ("k_bi_p", "m_bf16"): 50.36e6, ("k_bi_y", "m_bf16"): 79.29e6, ("k_bi_ay", "m_bf16"): 185.27e6,
+    ("k_bi_sz", "m_bf16"): 99.71e6, ("k_bi_az", "m_bf16"): 184.05e6, ("k_bi_xr", "m_bf16"): 109.35e6,
+    ("k_bi_py", "fp64"): 234.99e6,
+}
+
+
 def form_widths(form):
     # (M value bytes, preconditioned-vector bytes, index bytes)
     return {0: (8, 8, 4), 1: (4, 4, 2), 2: (2, 4, 2), 3: (4, 8, 2), 4: (2, 8, 2)}[form]
@@ -352,7 +362,9 @@ def main():
     assert len(names) == len(kms) == len(kbytes), (names, kms)
     roofline = {"bound": "hbm", "kernel": names[j],
                 "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 3),
-                "traffic": None, "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                "traffic": TRAFFIC_BYTES.get((names[j], args.form)),
+                "traffic_source": "profiles/iteration_kernels_128cube.md (ncu, one cold launch)",
+                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                 "kernel_ms": [round(v, 4) for v in kms],
                 "kernel_GBps": [round(kb / (v * 1e-3) / 1e9, 1) for kb, v in zip(kbytes, kms)]}
 

@@ -64,9 +64,16 @@ int main(int argc, char** argv) {
     cleanupMultiDCU(ctx);
     return EXIT_FAILURE;
   }
-  int iters = 0;
-  if (!precondOnly) iters = runBiCGSTABOnRank0(deviceMatrixA(ctx), &M);
+  int iters = 0, converged = 0, maxIters = 0;
+  double solverMs = 0.0, tol = 0.0;
+  if (!precondOnly) iters = runBiCGSTABOnRank0Info(deviceMatrixA(ctx), &M, &solverMs, &converged, &tol, &maxIters);
   printAlgoReport(algo.c_str(), numDCUUnits(ctx), useNnz ? "balanced_nnz" : "balanced_columns", ms, iters);
+  // Not printed by the reference: the solver's own numbers, for the results
+  // database (dcu_b200/results_db.py), on a line of its own so that scripts
+  // reading [ALGO_REPORT] are unaffected.
+  if (!precondOnly)
+    printf("[SOLVER_REPORT] gpupbicgstab_ms=%.4f, converged=%d, solver_tol=%.3e, max_iters=%d\n", solverMs, converged,
+           tol, maxIters);
   cudaFree(M.mPtr);
   cudaFree(M.mIndex);
   cudaFree(M.mData);

@@ -163,6 +163,15 @@ int numDCUUnits(MultiDCU_Context* ctx) { return ctx ? ctx->numDCUs : 0; }
 const char* lastErrorMultiDCU(MultiDCU_Context* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
 int runBiCGSTABOnRank0(CSC_Matrix* devA, CSC_Matrix* devM) {
+  return runBiCGSTABOnRank0Info(devA, devM, nullptr, nullptr, nullptr, nullptr);
+}
+
+int runBiCGSTABOnRank0Info(CSC_Matrix* devA, CSC_Matrix* devM, double* solverMs, int* converged, double* tol,
+                           int* maxIters) {
+  if (solverMs) *solverMs = 0.0;
+  if (converged) *converged = 0;
+  if (tol) *tol = 1e-7;
+  if (maxIters) *maxIters = 10000;
   if (!devA || !devM || devA->n <= 0 || devM->n != devA->n || devM->nonzeroes != devA->nonzeroes) return 0;
   const int n = devA->n;
   dcu_spai_ctx* s = nullptr;
@@ -191,6 +200,8 @@ int runBiCGSTABOnRank0(CSC_Matrix* devA, CSC_Matrix* devM) {
                          &info) == DCU_OK) {
         // a breakdown leaves NaN in the reference, whose loop then runs to MAX_ITER
         iters = (info.status == DCU_SOLVE_BREAKDOWN) ? opt.maxiter : info.iters;
+        if (solverMs) *solverMs = info.ms;
+        if (converged) *converged = info.status == DCU_SOLVE_CONVERGED;
       }
     }
   }

@@ -44,6 +44,14 @@ float RunDynamicSPAI_MultiDCU_MPI(MultiDCU_Context *ctx, const CSC_Matrix *CSC_A
  * arguments or a CUDA failure). */
 int runBiCGSTABOnRank0(CSC_Matrix *devCSC_A_full, CSC_Matrix *devCSC_M_global);
 
+/* runBiCGSTABOnRank0 that also reports the solve: device time in ms, whether
+ * it converged (0/1), the tolerance and the iteration cap it ran with (each
+ * output optional, NULL to skip).  Not in the reference: the command-line
+ * driver prints these on its [SOLVER_REPORT] line, which is where the
+ * experiment database takes the solver time from. */
+int runBiCGSTABOnRank0Info(CSC_Matrix *devCSC_A_full, CSC_Matrix *devCSC_M_global,
+                           double *solverMs, int *converged, double *tol, int *maxIters);
+
 /* src/spai_multi_dcu.cpp:1486-1551: copies host A to the device.  Optional
  * here (Run* uploads A itself); kept for callers that follow the reference's
  * call order.  The device copy is reachable through deviceMatrixA(ctx). */

@@ -259,7 +259,9 @@ int dcu_batch_solve_d(dcu_spai_ctx* ctx, int nsys, const int* sys_off, int n, in
                       dcu_build_info* binfo, dcu_solve_info* sinfo);
 
 /* Diagnostic timing: re-launch each iteration kernel of the last solve on
- * this context `reps` times on that solve's buffers and write the mean device
+ * this context `reps` times on that solve's buffers, each timed launch right
+ * after an untimed launch of the kernel that precedes it in the iteration (so
+ * the L2 cache holds what it holds in a solve), and write the mean device
  * time per launch (ms) to ms_out[0..count-1], in launch order.  With an FP64
  * preconditioner the iteration runs five fused kernels:
  *   p/y = M p | A y + (r*, Ay) | s/z = M s | A z + dots | x/r update + dots

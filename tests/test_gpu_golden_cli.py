@@ -59,3 +59,23 @@ def test_cli_algo_report(tmp_path, algo):
     out2 = subprocess.run([N.CLI_PATH, "--matrix", str(path), "--precondition-only"], capture_output=True,
                           text=True, timeout=120)
     assert out2.returncode == 0 and "iteration_count=0" in out2.stdout
+
+
+def test_results_db_records_cli_runs(tmp_path):
+    """`record` runs the driver (both partitions) and stores what it printed."""
+    from dcu_b200 import results_db as R
+
+    A = W.convdiff2d(64, 10.0)
+    path = tmp_path / "cd2d.mtx"
+    write_mtx(str(path), A)
+    db = str(tmp_path / "runs.sqlite")
+    assert R.main(["record", "--db", db, "--matrix", str(path), "--tag", "gpu"]) == 0
+    with R.connect(db) as conn:
+        rows = conn.execute("SELECT er.run_tag, er.matrix_rows, er.matrix_nnz, ram.iteration_count, ram.converged, "
+                            "ram.preconditioner_ms, ram.gpupbicgstab_ms FROM run_algorithm_metrics ram "
+                            "JOIN experiment_runs er ON er.id = ram.run_id ORDER BY er.run_tag").fetchall()
+    assert [r["run_tag"] for r in rows] == ["gpu-dynamic", "gpu-static"]
+    for r in rows:
+        assert (r["matrix_rows"], r["matrix_nnz"]) == (A.n, A.nnz)
+        assert abs(r["iteration_count"] - GOLDEN["convdiff2d_64_pe10"]["iters_reference_settings"]) <= 1
+        assert r["converged"] == 1 and r["preconditioner_ms"] > 0 and r["gpupbicgstab_ms"] > 0
