@@ -54,6 +54,8 @@ struct BArgs {
   const int* tile_row0;           // [ntiles]
   const int* tile_off;            // [nsys + 1] first tile of each system
   const long long* off;
+  const int* kd;                  // per (slice, k) offset descriptors
+  const int* su;                  // per slice: all of its k uniform
   const int* ix;
   const double* aval;
   const double* mval;
@@ -75,8 +77,11 @@ struct BArgs {
 };
 
 // out[q] = sum_k val * X[col][q], q < R, X row-major with R columns.
+// A slice whose every k has one column offset (su, kd: SellPlan) forms its
+// columns from the row and reads no index.
 template <int R, typename F>
-__device__ __forceinline__ void sell_row_multi(const long long* __restrict__ off, const double* __restrict__ val,
+__device__ __forceinline__ void sell_row_multi(const long long* __restrict__ off, const int* __restrict__ kd,
+                                               const int* __restrict__ su, const double* __restrict__ val,
                                                const int* __restrict__ ix, int row, F xf, double (&out)[R]) {
 #pragma unroll
   for (int q = 0; q < R; ++q) out[q] = 0.0;
@@ -84,10 +89,12 @@ __device__ __forceinline__ void sell_row_multi(const long long* __restrict__ off
   const long long o0 = __ldg(off + sl), o1 = __ldg(off + sl + 1);
   const long long base = o0 + (row & 31);
   const int w = (int)((o1 - o0) >> 5);
+  const bool uniform = __ldg(su + sl) != 0;
+  const int* __restrict__ kp = kd + (o0 >> 5);
   for (int k = 0; k < w; ++k) {
     const long long qk = base + 32ll * k;
     const double a = __ldcs(val + qk);
-    const int c = __ldcs(ix + qk);
+    const int c = uniform ? row + (__ldg(kp + k) >> 1) : __ldcs(ix + qk);
     double xv[R];
     xf(c, xv);
 #pragma unroll
@@ -170,7 +177,7 @@ __global__ void __launch_bounds__(BT) kb_init(BArgs<R> a, double tol, int tol_mo
   double v[3][R] = {};
   if (valid) {
     double ax[R], bb[R];
-    sell_row_multi<R>(a.off, a.aval, a.ix, row, [&](int c, double (&o)[R]) { load_row<R>(a.x, c, o); }, ax);
+    sell_row_multi<R>(a.off, a.kd, a.su, a.aval, a.ix, row, [&](int c, double (&o)[R]) { load_row<R>(a.x, c, o); }, ax);
     load_row<R>(a.b, row, bb);
 #pragma unroll
     for (int q = 0; q < R; ++q) {
@@ -236,7 +243,7 @@ __global__ void __launch_bounds__(BT) kb_py(BArgs<R> a) {
     for (int q = 0; q < R; ++q) o[q] = rr[q] + beta[q] * (pp[q] - omega[q] * yy[q]);
   };
   double yv[R], pv[R];
-  sell_row_multi<R>(a.off, a.mval, a.ix, row, pf, yv);
+  sell_row_multi<R>(a.off, a.kd, a.su, a.mval, a.ix, row, pf, yv);
   pf(row, pv);
 #pragma unroll
   for (int q = 0; q < R; ++q) {
@@ -255,7 +262,7 @@ __global__ void __launch_bounds__(BT) kb_ay(BArgs<R> a) {
   double v[1][R] = {};
   if (row < a.sys_off[sys + 1]) {
     double ayv[R], rsv[R];
-    sell_row_multi<R>(a.off, a.aval, a.ix, row, [&](int c, double (&o)[R]) { load_row<R>(a.y, c, o); }, ayv);
+    sell_row_multi<R>(a.off, a.kd, a.su, a.aval, a.ix, row, [&](int c, double (&o)[R]) { load_row<R>(a.y, c, o); }, ayv);
     load_row<R>(a.rs, row, rsv);
 #pragma unroll
     for (int q = 0; q < R; ++q) {
@@ -301,7 +308,7 @@ __global__ void __launch_bounds__(BT) kb_sz(BArgs<R> a) {
     for (int q = 0; q < R; ++q) o[q] = rr[q] + nalpha[q] * yy[q];
   };
   double zv[R], sv[R];
-  sell_row_multi<R>(a.off, a.mval, a.ix, row, sf, zv);
+  sell_row_multi<R>(a.off, a.kd, a.su, a.mval, a.ix, row, sf, zv);
   sf(row, sv);
 #pragma unroll
   for (int q = 0; q < R; ++q) {
@@ -320,7 +327,7 @@ __global__ void __launch_bounds__(BT) kb_az(BArgs<R> a) {
   double v[2][R] = {};
   if (row < a.sys_off[sys + 1]) {
     double azv[R], sv[R];
-    sell_row_multi<R>(a.off, a.aval, a.ix, row, [&](int c, double (&o)[R]) { load_row<R>(a.z, c, o); }, azv);
+    sell_row_multi<R>(a.off, a.kd, a.su, a.aval, a.ix, row, [&](int c, double (&o)[R]) { load_row<R>(a.z, c, o); }, azv);
     load_row<R>(a.s, row, sv);
 #pragma unroll
     for (int q = 0; q < R; ++q) {
@@ -466,12 +473,15 @@ int run_batch(Ctx* c, int nsys, const int* sys_off_d, const SellPlan& plan, cons
                        al(sizeof(int) * 3 * pairs) + al(sizeof(int) * (size_t)nsys) + al(sizeof(BGlobal));
   DCU_TRY(ensure(c, B_VEC, 9 * vec + small));
   char* p = bp<char>(c, B_VEC);
-  BArgs<R> a{};
+  BArgs<R> a;
+  std::memset(&a, 0, sizeof(a));  // padding included: the struct keys the graph cache
   a.n = n;
   a.nsys = nsys;
   a.ntiles = ntiles;
   a.sys_off = sys_off_d;
   a.off = plan.off;
+  a.kd = plan.kd;
+  a.su = plan.su;
   a.ix = plan.idx;
   a.aval = aval;
   a.mval = mval;
@@ -515,8 +525,8 @@ int run_batch(Ctx* c, int nsys, const int* sys_off_d, const SellPlan& plan, cons
   kb_init<R><<<ntiles, BT, 0, c->stream>>>(a, opt->tol, opt->tol_mode);
   DCU_LAUNCHED(c, "kb_init");
   // the first iteration starts with p = r: beta = 0 and p, ay zero-filled
-  std::vector<const void*> key = {(const void*)&kb_py<R>, plan.off, aval, mval, B, X, p, (const void*)(intptr_t)n,
-                                  (const void*)(intptr_t)nsys, (const void*)(intptr_t)ntiles};
+  std::vector<const void*> key = {(const void*)&kb_py<R>, (const void*)(intptr_t)ntiles};
+  key_append(key, a);
   GraphSlot* ge = nullptr;
   for (auto& e : c->graphs)
     if (e.key == key) ge = &e;

@@ -62,15 +62,40 @@ __device__ __forceinline__ double ldv(const T* p) { return (double)__ldg(p); }
 // One SELL-32 row: sum_k val[q] * xf(col[q]).  A warp covers one slice, so
 // each k step reads 32 consecutive slots.  Slots are taken 8 at a time with
 // every value and index load issued before the dependent gathers, so a thread
-// keeps up to 16 independent loads in flight.
+// keeps up to 16 independent loads in flight.  A slice whose every k has one
+// column offset for all its rows (su[s]; SellPlan::kd) reads no index at all:
+// the column is the row plus the slice's offset, one broadcast load per k
+// from a table 1/32 the size of the index array.
 template <typename MT, typename IT, typename F>
-__device__ __forceinline__ double sell_row(const long long* __restrict__ off, const MT* __restrict__ val,
+__device__ __forceinline__ double sell_row(const long long* __restrict__ off, const int* __restrict__ kd,
+                                           const int* __restrict__ su, const MT* __restrict__ val,
                                            const IT* __restrict__ ix, int r, F xf) {
   const int s = r >> 5;
   const long long o0 = __ldg(off + s), o1 = __ldg(off + s + 1);
   const long long base = o0 + (r & 31);
   const int w = (int)((o1 - o0) >> 5);
   double acc = 0.0;
+  if (__ldg(su + s)) {
+    const int* __restrict__ kp = kd + (o0 >> 5);
+    for (int k0 = 0; k0 < w; k0 += 8) {
+      double av[8];
+      int cv[8];
+#pragma unroll
+      for (int t = 0; t < 8; ++t) {
+        if (k0 + t < w) {
+          av[t] = ldm(val + base + 32ll * (k0 + t));
+          cv[t] = r + (__ldg(kp + k0 + t) >> 1);
+        } else {
+          av[t] = 0.0;
+          cv[t] = r;
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < 8; ++t)
+        if (k0 + t < w) acc += av[t] * xf(cv[t]);
+    }
+    return acc;
+  }
   for (int k0 = 0; k0 < w; k0 += 8) {
     double av[8];
     int cv[8];
@@ -145,6 +170,8 @@ template <typename MT, typename IT, typename VT>
 struct BiArgs {
   int n;
   const long long* off;
+  const int* kd;        // per (slice, k) offset descriptors (SellPlan::kd)
+  const int* su;        // per slice: all of its k uniform (SellPlan::su)
   const IT* ix;         // shared by A and M (same pattern)
   const double* aval;
   const MT* mval;
@@ -179,7 +206,7 @@ __global__ void __launch_bounds__(BI_BLOCK) k_bi_init(BiArgs<MT, IT, VT> a, doub
   double v[3] = {0.0, 0.0, 0.0};
   const int stride = gridDim.x * BI_BLOCK;
   for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) {
-    const double ax = sell_row(a.off, a.aval, a.ix, r, [&](int c) { return ldv(a.x + c); });
+    const double ax = sell_row(a.off, a.kd, a.su, a.aval, a.ix, r, [&](int c) { return ldv(a.x + c); });
     const double br = a.b[r];
     const double rr = br + (-1.0) * ax;
     a.r[r] = rr;
@@ -234,7 +261,7 @@ __global__ void __launch_bounds__(BI_BLOCK) k_bi_py(BiArgs<MT, IT, VT> a) {
   auto pf = [&](int c) { return ldv(rr + c) + beta * (ldv(pold + c) - omega * ldv(ay + c)); };
   const int stride = gridDim.x * BI_BLOCK;
   for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) {
-    const double yv = sell_row(a.off, a.mval, a.ix, r, pf);
+    const double yv = sell_row(a.off, a.kd, a.su, a.mval, a.ix, r, pf);
     pnew[r] = (VT)pf(r);
     a.y[r] = (VT)yv;
   }
@@ -290,7 +317,7 @@ __global__ void __launch_bounds__(BI_BLOCK, 8) k_bi_y(BiArgs<MT, IT, VT> a) {
   const VT* __restrict__ p = a.p0;
   const int stride = gridDim.x * BI_BLOCK;
   for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride)
-    a.y[r] = (VT)sell_row(a.off, a.mval, a.ix, r, [&](int c) { return ldv(p + c); });
+    a.y[r] = (VT)sell_row(a.off, a.kd, a.su, a.mval, a.ix, r, [&](int c) { return ldv(p + c); });
 }
 
 // K2: ay = A y; alpha = rho / (r*, ay)
@@ -301,7 +328,7 @@ __global__ void __launch_bounds__(BI_BLOCK) k_bi_ay(BiArgs<MT, IT, VT> a) {
   const VT* __restrict__ y = a.y;
   const int stride = gridDim.x * BI_BLOCK;
   for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) {
-    const double ayv = sell_row(a.off, a.aval, a.ix, r, [&](int c) { return ldv(y + c); });
+    const double ayv = sell_row(a.off, a.kd, a.su, a.aval, a.ix, r, [&](int c) { return ldv(y + c); });
     a.ay[r] = ayv;
     v[0] += (double)a.rs[r] * ayv;
   }
@@ -327,7 +354,7 @@ __global__ void __launch_bounds__(BI_BLOCK) k_bi_sz(BiArgs<MT, IT, VT> a) {
   auto sf = [&](int c) { return ldv(rr + c) + nalpha * ldv(ay + c); };
   const int stride = gridDim.x * BI_BLOCK;
   for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) {
-    const double zv = sell_row(a.off, a.mval, a.ix, r, sf);
+    const double zv = sell_row(a.off, a.kd, a.su, a.mval, a.ix, r, sf);
     a.s[r] = rr[r] + nalpha * ay[r];
     a.z[r] = (VT)zv;
   }
@@ -341,7 +368,7 @@ __global__ void __launch_bounds__(BI_BLOCK) k_bi_az(BiArgs<MT, IT, VT> a) {
   const VT* __restrict__ z = a.z;
   const int stride = gridDim.x * BI_BLOCK;
   for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) {
-    const double azv = sell_row(a.off, a.aval, a.ix, r, [&](int c) { return ldv(z + c); });
+    const double azv = sell_row(a.off, a.kd, a.su, a.aval, a.ix, r, [&](int c) { return ldv(z + c); });
     a.az[r] = azv;
     v[0] += azv * a.s[r];
     v[1] += azv * azv;
@@ -430,7 +457,7 @@ __global__ void __launch_bounds__(BI_BLOCK) k_bi_true(BiArgs<MT, IT, VT> a, int 
   double v[2] = {0.0, 0.0};
   const int stride = gridDim.x * BI_BLOCK;
   for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) {
-    const double ax = sell_row(a.off, a.aval, a.ix, r, [&](int c) { return ldv(a.x + c); });
+    const double ax = sell_row(a.off, a.kd, a.su, a.aval, a.ix, r, [&](int c) { return ldv(a.x + c); });
     const double rt = a.b[r] - ax;
     if (replace) a.r[r] = rt;
     v[0] += (double)a.rs[r] * rt;
@@ -508,8 +535,11 @@ int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval,
   DCU_TRY(ensure(c, B_SCAL, sizeof(Scal)));
   char* base = bp<char>(c, B_VEC);
   BiArgs<MT, IT, VT> a;
+  std::memset(&a, 0, sizeof(a));  // padding included: the struct keys the graph cache
   a.n = n;
   a.off = plan.off;
+  a.kd = plan.kd;
+  a.su = plan.su;
   a.ix = ix;
   a.aval = aval;
   a.mval = mval;
@@ -537,8 +567,11 @@ int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval,
   // graph of CHUNK_ITERS iterations
   // the key names the kernel instantiation too: the same buffers are reused
   // by every precision form
-  std::vector<const void*> key = {(const void*)&k_bi_py<MT, IT, VT>, plan.off, ix, aval, mval, b, x, base, a.part,
-                                  a.S, (const void*)(intptr_t)n, (const void*)(intptr_t)grid};
+  std::vector<const void*> key = {(const void*)&k_bi_py<MT, IT, VT>, (const void*)(intptr_t)grid,
+                                  (const void*)(intptr_t)g_py, (const void*)(intptr_t)g_ay, (const void*)(intptr_t)g_sz,
+                                  (const void*)(intptr_t)g_az, (const void*)(intptr_t)g_xr, (const void*)(intptr_t)g_p,
+                                  (const void*)(intptr_t)g_y};
+  key_append(key, a);
   GraphSlot* ge = nullptr;
   for (auto& e : c->graphs)
     if (e.key == key) ge = &e;

@@ -9,6 +9,7 @@
 #include <cstring>
 #include <functional>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "dcu_spai.h"
@@ -41,6 +42,7 @@ enum BufId {
   B_SELL_IDX,      // SELL absolute column indices
   B_SELL_DEL,      // SELL 16-bit column deltas
   B_SELL_PERM,     // SELL slot -> CSC position (-1 padding)
+  B_SELL_KD,       // SELL per (slice, k) column-offset descriptors
   B_SELL_AVAL,     // A values in SELL order (FP64)
   B_SELL_MVAL,     // M values in SELL order (FP64 / FP32 / BF16)
   B_VEC,           // solver vectors
@@ -53,6 +55,18 @@ enum BufId {
 };
 
 // An instantiated CUDA graph and the buffers/sizes it was captured with.
+// Appends the bytes of a trivially copyable value (zero-filled first, so
+// padding compares equal) to a graph-cache key.  Keying a graph on the whole
+// argument struct its kernels captured means any changed pointer, size or
+// scalar gives a new graph: a reallocated buffer never reaches a stale one.
+template <typename T>
+void key_append(std::vector<const void*>& key, const T& v) {
+  static_assert(std::is_trivially_copyable<T>::value, "graph keys copy bytes");
+  uintptr_t w[(sizeof(T) + sizeof(uintptr_t) - 1) / sizeof(uintptr_t)] = {};
+  std::memcpy(w, &v, sizeof(T));
+  for (uintptr_t u : w) key.push_back(reinterpret_cast<const void*>(u));
+}
+
 struct GraphSlot {
   std::vector<const void*> key;
   cudaGraphExec_t exec = nullptr;
@@ -129,6 +143,11 @@ struct SellPlan {
   const int* idx = nullptr;
   const int16_t* del = nullptr;
   const int* perm = nullptr;
+  // One int per (slice, k), at kd[off[s] / 32 + k]: (d << 1) | 1 when every
+  // row of the slice has its k-th entry at column row + d, else 0.  A warp
+  // then forms the column from the row and skips the per-slot index load.
+  const int* kd = nullptr;
+  const int* su = nullptr;  // per slice: 1 when every kd of the slice is uniform
 };
 
 // Fails with DCU_ERR_ARG unless ptr[0] = 0, ptr is non-decreasing,

@@ -10,6 +10,7 @@
 //          reads 32 consecutive slots per k (128-byte lines for FP32/int32,
 //          256 bytes for FP64).  Padding slots carry column = r and perm = -1.
 //          del int16 holds col - r when every |col - r| < 32768.
+#include <climits>
 #include <mutex>
 
 #include "internal.cuh"
@@ -209,32 +210,57 @@ __global__ void k_sell_width(const int* __restrict__ rptr, int n, int nslices, i
   }
 }
 
+// One warp per slice (rows 32 s .. 32 s + 31 on the lanes).  First try the
+// offset-aligned layout: slot k of every row holds the entry at the k-th
+// smallest column offset (column - row) found in the slice, or a zero-valued
+// padding slot at that offset.  It fits when the slice has no more distinct
+// offsets than its longest row has entries (every stencil slice away from the
+// domain's first row), and then every k has one offset for the whole slice.
+// Otherwise the compact layout: row entries in order, padding at the end.
+// Rows keep their column order either way; padding slots have perm = -1 and,
+// in the compact layout or where row + offset leaves [0, n), column = row.
 __global__ void k_sell_fill(const int* __restrict__ rptr, const int* __restrict__ rcol, const int* __restrict__ rperm,
                             int n, int nslices, const long long* __restrict__ off, int* __restrict__ sidx,
                             int* __restrict__ sperm, int* __restrict__ maxdelta) {
-  int rows_total = nslices * 32;
+  const int rows_total = nslices * 32;
   int local_max = 0;
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows_total; r += gridDim.x * blockDim.x) {
-    int s = r >> 5, lane = r & 31;
-    long long base = off[s] + lane;
-    int w = (int)((off[s + 1] - off[s]) >> 5);
+    const int s = r >> 5, lane = r & 31;
+    const long long base = off[s] + lane;
+    const int w = (int)((off[s + 1] - off[s]) >> 5);
     int rs = 0, len = 0;
     if (r < n) {
       rs = rptr[r];
       len = rptr[r + 1] - rs;
     }
-    int self = (r < n) ? r : 0;
+    const int self = (r < n) ? r : 0;
+    for (int j = 0; j < len; ++j) local_max = max(local_max, abs(rcol[rs + j] - self));
+    int i = 0;
     for (int k = 0; k < w; ++k) {
-      long long q = base + 32ll * k;
-      if (k < len) {
-        int col = rcol[rs + k];
-        sidx[q] = col;
-        sperm[q] = rperm[rs + k];
-        int d = abs(col - self);
-        local_max = max(local_max, d);
+      const int cand = (i < len) ? rcol[rs + i] - r : INT_MAX;
+      const int m = __reduce_min_sync(0xffffffffu, cand);
+      const long long q = base + 32ll * k;
+      if (i < len && cand == m) {
+        sidx[q] = rcol[rs + i];
+        sperm[q] = rperm[rs + i];
+        ++i;
       } else {
-        sidx[q] = self;
+        int c = self;
+        if (r < n && m != INT_MAX && (long long)r + m >= 0 && (long long)r + m < n) c = r + m;
+        sidx[q] = c;
         sperm[q] = -1;
+      }
+    }
+    if (!__all_sync(0xffffffffu, i == len)) {
+      for (int k = 0; k < w; ++k) {
+        const long long q = base + 32ll * k;
+        if (k < len) {
+          sidx[q] = rcol[rs + k];
+          sperm[q] = rperm[rs + k];
+        } else {
+          sidx[q] = self;
+          sperm[q] = -1;
+        }
       }
     }
   }
@@ -257,6 +283,30 @@ __global__ void k_sell_delta(const int* __restrict__ sidx, long long slots, int 
       long long q = base + 32ll * k;
       del[q] = (int16_t)(sidx[q] - self);
     }
+  }
+}
+
+// One warp per slice (rows 32 s .. 32 s + 31 on the lanes): for every k,
+// whether all of the slice's rows below n have their k-th slot at the same
+// offset d = column - row.  Rows past n (last slice) never run and do not
+// count.  Writes kd[off[s] / 32 + k] = (d << 1) | 1, or 0, and su[s] = 1 when
+// every k of the slice has one offset (the SpMV then reads no index at all).
+__global__ void k_sell_desc(const int* __restrict__ sidx, int n, int nslices, const long long* __restrict__ off,
+                            int* __restrict__ kd, int* __restrict__ su) {
+  const int rows_total = nslices * 32;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows_total; r += gridDim.x * blockDim.x) {
+    const int s = r >> 5, lane = r & 31;
+    const long long o0 = off[s];
+    const int w = (int)((off[s + 1] - o0) >> 5);
+    bool all = true;
+    for (int k = 0; k < w; ++k) {
+      const int d = sidx[o0 + 32ll * k + lane] - r;
+      const int d0 = __shfl_sync(0xffffffffu, d, 0);  // row 32 s < n always
+      const bool same = __all_sync(0xffffffffu, r >= n || d == d0);
+      all = all && same;
+      if (lane == 0) kd[(o0 >> 5) + k] = same ? (int)(((unsigned)d0 << 1) | 1u) : 0;
+    }
+    if (lane == 0) su[s] = all ? 1 : 0;
   }
 }
 
@@ -443,6 +493,13 @@ int sell_fill_from_csr(Ctx* c, int n, int nnz, const int* rptr, const int* rcol,
     DCU_LAUNCHED(c, "k_sell_delta");
     plan->del = del;
   }
+  DCU_TRY(ensure(c, B_SELL_KD, sizeof(int) * ((size_t)nslices + (size_t)(slots / 32) + 1)));
+  int* su = bp<int>(c, B_SELL_KD);
+  int* kd = su + nslices;
+  k_sell_desc<<<waves_grid(c, (long long)nslices * 32, 256, 8), 256, 0, c->stream>>>(sidx, n, nslices, off, kd, su);
+  DCU_LAUNCHED(c, "k_sell_desc");
+  plan->kd = kd;
+  plan->su = su;
   plan->n = n;
   plan->nnz = nnz;
   plan->nslices = nslices;
