@@ -57,18 +57,25 @@ def iteration_kernels(w_m):
     return k1 + ["k_bi_ay", "k_bi_sz", "k_bi_az", "k_bi_xr"]
 
 
-def bytes_per_kernel(n, nnz, w_m, w_v, w_i):
+def index_bytes(n, w_i, slots, uniform_slots):
+    """Bytes of column information one SpMV reads: the per-slot index in
+    slices that are not offset-uniform, one 4-byte offset per entry position
+    of the uniform ones, and the slice offset + flag (12 bytes per slice)."""
+    return w_i * (slots - uniform_slots) + 4 * (uniform_slots // 32) + 12 * ((n + 31) // 32)
+
+
+def bytes_per_kernel(n, nnz, w_m, w_v, ib):
     """Algorithmic HBM bytes of each iteration kernel (one launch), in the
-    order of iteration_kernels()."""
+    order of iteration_kernels(); ib = index_bytes() of one SpMV."""
     if w_m < 8:
         k1 = [n * (16 + 2 * w_v),                           # K1a p = r + beta(p - w ay)
-              nnz * (w_m + w_i) + n * 2 * w_v]              # K1b y = M p
+              nnz * w_m + ib + n * 2 * w_v]                 # K1b y = M p
     else:
-        k1 = [nnz * (w_m + w_i) + n * (16 + 3 * w_v)]      # K1 p on the fly, y = M p
+        k1 = [nnz * w_m + ib + n * (16 + 3 * w_v)]         # K1 p on the fly, y = M p
     return k1 + [
-        nnz * (8 + w_i) + n * (8 + 2 * w_v),      # K2 ay = A y, (r*, ay)
-        nnz * (w_m + w_i) + n * (24 + w_v),       # K3 s = r - alpha ay, z = M s
-        nnz * (8 + w_i) + n * (16 + w_v),         # K4 az = A z, (az, s), (az, az)
+        nnz * 8 + ib + n * (8 + 2 * w_v),         # K2 ay = A y, (r*, ay)
+        nnz * w_m + ib + n * (24 + w_v),          # K3 s = r - alpha ay, z = M s
+        nnz * 8 + ib + n * (16 + w_v),            # K4 az = A z, (az, s), (az, az)
         n * (40 + 3 * w_v),                       # K5 x, r update, (r*, r), (r, r)
     ]
 
@@ -77,9 +84,9 @@ def bytes_per_kernel(n, nnz, w_m, w_v, w_i):
 # from one ncu capture per kernel (profiles/iteration_kernels_128cube.md;
 # cold L2, single launch), keyed by (kernel, form).
 TRAFFIC_BYTES = {
-    ("k_bi_p", "m_bf16"): 50.36e6, ("k_bi_y", "m_bf16"): 79.29e6, ("k_bi_ay", "m_bf16"): 185.27e6,
-    ("k_bi_sz", "m_bf16"): 99.71e6, ("k_bi_az", "m_bf16"): 184.05e6, ("k_bi_xr", "m_bf16"): 109.35e6,
-    ("k_bi_py", "fp64"): 234.99e6,
+    ("k_bi_p", "m_bf16"): 50.38e6, ("k_bi_y", "m_bf16"): 49.64e6, ("k_bi_ay", "m_bf16"): 157.94e6,
+    ("k_bi_sz", "m_bf16"): 70.32e6, ("k_bi_az", "m_bf16"): 158.15e6, ("k_bi_xr", "m_bf16"): 110.28e6,
+    ("k_bi_py", "fp64"): 178.59e6,
 }
 
 
@@ -349,7 +356,8 @@ def main():
     # per-kernel timing of the headline form's iteration kernels (after its solve)
     kms = ctx.profile_iteration(reps=20)
     w_m, w_v, w_i = form_widths(head)
-    kbytes = bytes_per_kernel(n, nnz, w_m, w_v, w_i)
+    slots, uslots = ctx.sell_plan_stats()
+    kbytes = bytes_per_kernel(n, nnz, w_m, w_v, index_bytes(n, w_i, slots, uslots))
     j = int(np.argmax(kms))
     peaks = {}
     try:
@@ -366,7 +374,12 @@ def main():
                 "traffic_source": "profiles/iteration_kernels_128cube.md (ncu, one cold launch)",
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                 "kernel_ms": [round(v, 4) for v in kms],
-                "kernel_GBps": [round(kb / (v * 1e-3) / 1e9, 1) for kb, v in zip(kbytes, kms)]}
+                "kernel_GBps": [round(kb / (v * 1e-3) / 1e9, 1) for kb, v in zip(kbytes, kms)],
+                "sell_slots": slots, "uniform_slots": uslots}
+    it_us = inf_head[-1][1].ms * 1e3 / max(1, inf_head[-1][1].iters)
+    it_gbs = sum(kbytes) / (it_us * 1e-6) / 1e9
+    roofline["iteration"] = {"bytes": int(sum(kbytes)), "us": round(it_us, 1), "achieved": round(it_gbs, 1),
+                             "frac": round(it_gbs / peak, 3)}
 
     # end to end through the host-buffer entry point
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()

@@ -156,6 +156,12 @@ class Context:
         self._check(self._L.dcu_profile_iteration_kernels(self.h, reps, ms, 16, C.byref(cnt)))
         return [float(ms[i]) for i in range(cnt.value)]
 
+    def sell_plan_stats(self):
+        """(slots, uniform_slots) of the last SELL layout built on this context."""
+        s, u = C.c_longlong(), C.c_longlong()
+        self._check(self._L.dcu_sell_plan_stats(self.h, C.byref(s), C.byref(u)))
+        return s.value, u.value
+
     def csc_to_csr_d(self, n, nnz, ptr_d, idx_d, val_d, rptr_d, ridx_d, rval_d):
         self._check(self._L.dcu_csc_to_csr_d(self.h, n, nnz, _p(ptr_d), _p(idx_d), _p(val_d), _p(rptr_d),
                                              _p(ridx_d), _p(rval_d)))

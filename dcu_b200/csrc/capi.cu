@@ -475,6 +475,12 @@ int dcu_batch_solve_d(dcu_spai_ctx* c, int nsys, const int* sys_off, int n, int 
   }
 }
 
+int dcu_sell_plan_stats(dcu_spai_ctx* c, long long* slots, long long* uniform_slots) {
+  if (!c) return DCU_ERR_ARG;
+  StreamScope scope(c);
+  return dcu::plan_stats(c, slots, uniform_slots);
+}
+
 int dcu_profile_iteration_kernels(dcu_spai_ctx* c, int reps, float* ms_out, int cap, int* count) {
   if (!c || !ms_out) return DCU_ERR_ARG;
   StreamScope scope(c);

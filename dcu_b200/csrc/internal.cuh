@@ -51,6 +51,7 @@ enum BufId {
   B_UPLOAD,        // host-API uploads
   B_SORTTMP,       // global scratch of the long-row sort
   B_FBLIST,        // columns handed from the thread kernel to the group kernel
+  B_PLANSTAT,      // slots of the last SELL plan in offset-uniform slices
   B_COUNT
 };
 
@@ -149,6 +150,9 @@ struct SellPlan {
   const int* kd = nullptr;
   const int* su = nullptr;  // per slice: 1 when every kd of the slice is uniform
 };
+
+// Slot counts of the last SELL plan built on a context (diagnostics).
+int plan_stats(Ctx* c, long long* slots, long long* uniform_slots);
 
 // Fails with DCU_ERR_ARG unless ptr[0] = 0, ptr is non-decreasing,
 // ptr[n] = nnz and every row index lies in [0, n).  Every entry point runs it

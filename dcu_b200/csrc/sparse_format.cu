@@ -292,7 +292,7 @@ __global__ void k_sell_delta(const int* __restrict__ sidx, long long slots, int 
 // count.  Writes kd[off[s] / 32 + k] = (d << 1) | 1, or 0, and su[s] = 1 when
 // every k of the slice has one offset (the SpMV then reads no index at all).
 __global__ void k_sell_desc(const int* __restrict__ sidx, int n, int nslices, const long long* __restrict__ off,
-                            int* __restrict__ kd, int* __restrict__ su) {
+                            int* __restrict__ kd, int* __restrict__ su, unsigned long long* __restrict__ uslots) {
   const int rows_total = nslices * 32;
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows_total; r += gridDim.x * blockDim.x) {
     const int s = r >> 5, lane = r & 31;
@@ -306,7 +306,10 @@ __global__ void k_sell_desc(const int* __restrict__ sidx, int n, int nslices, co
       all = all && same;
       if (lane == 0) kd[(o0 >> 5) + k] = same ? (int)(((unsigned)d0 << 1) | 1u) : 0;
     }
-    if (lane == 0) su[s] = all ? 1 : 0;
+    if (lane == 0) {
+      su[s] = all ? 1 : 0;
+      if (all && w > 0) atomicAdd(uslots, 32ull * (unsigned long long)w);
+    }
   }
 }
 
@@ -496,7 +499,12 @@ int sell_fill_from_csr(Ctx* c, int n, int nnz, const int* rptr, const int* rcol,
   DCU_TRY(ensure(c, B_SELL_KD, sizeof(int) * ((size_t)nslices + (size_t)(slots / 32) + 1)));
   int* su = bp<int>(c, B_SELL_KD);
   int* kd = su + nslices;
-  k_sell_desc<<<waves_grid(c, (long long)nslices * 32, 256, 8), 256, 0, c->stream>>>(sidx, n, nslices, off, kd, su);
+  DCU_TRY(ensure(c, B_PLANSTAT, 2 * sizeof(unsigned long long)));
+  unsigned long long* pst = bp<unsigned long long>(c, B_PLANSTAT);
+  const unsigned long long hst[2] = {(unsigned long long)slots, 0ull};
+  DCU_CUDA(c, cudaMemcpyAsync(pst, hst, sizeof(hst), cudaMemcpyHostToDevice, c->stream));
+  k_sell_desc<<<waves_grid(c, (long long)nslices * 32, 256, 8), 256, 0, c->stream>>>(sidx, n, nslices, off, kd, su,
+                                                                                       pst + 1);
   DCU_LAUNCHED(c, "k_sell_desc");
   plan->kd = kd;
   plan->su = su;
@@ -523,6 +531,16 @@ int sell_plan_rows(Ctx* c, int n, int nnz, const int* rptr, const int* rcol, Sel
     DCU_LAUNCHED(c, "k_iota");
   }
   return sell_fill_from_csr(c, n, nnz, rptr, rcol, rperm, plan);
+}
+
+int plan_stats(Ctx* c, long long* slots, long long* uniform_slots) {
+  if (!c->buf[B_PLANSTAT].p) return fail(c, DCU_ERR_ARG, "no SELL plan has been built on this context");
+  unsigned long long h[2] = {0, 0};
+  DCU_CUDA(c, cudaMemcpyAsync(h, c->buf[B_PLANSTAT].p, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  DCU_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (slots) *slots = (long long)h[0];
+  if (uniform_slots) *uniform_slots = (long long)h[1];
+  return DCU_OK;
 }
 
 int sell_gather_f64(Ctx* c, const SellPlan& p, const double* src, double* dst) { return sell_gather<double>(c, p, src, dst); }

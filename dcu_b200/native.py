@@ -73,6 +73,7 @@ SIGNATURES = {
     "dcu_batch_solve_d": (_i, [_vp, _i, _vp, _i, _i, _vp, _vp, _vp, _i, _vp, _vp, _OPT, _vp, _vp, _vp,
                                C.POINTER(BuildInfo), C.POINTER(SolveInfo)]),
     "dcu_profile_iteration_kernels": (_i, [_vp, _i, C.POINTER(C.c_float), _i, C.POINTER(_i)]),
+    "dcu_sell_plan_stats": (_i, [_vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     "dcu_mtx_read": (_i, [C.c_char_p, C.POINTER(_i), C.POINTER(_i), C.POINTER(C.POINTER(_i)),
                           C.POINTER(C.POINTER(_i)), C.POINTER(C.POINTER(C.c_double))]),
     "dcu_mtx_free": (None, [_vp]),

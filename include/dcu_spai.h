@@ -271,6 +271,13 @@ int dcu_batch_solve_d(dcu_spai_ctx* ctx, int nsys, const int* sys_off, int n, in
  * smaller.  The solver vectors and x are left in an unspecified state. */
 int dcu_profile_iteration_kernels(dcu_spai_ctx* ctx, int reps, float* ms_out, int cap, int* count);
 
+/* Diagnostics of the last SELL-32 layout built on this context (by any solve
+ * that runs BiCGSTAB): *slots = slots including padding, *uniform_slots =
+ * slots in slices whose every entry position has one column offset for all
+ * 32 rows (those slices read no index array).  Either output may be NULL.
+ * No counterpart in the reference. */
+int dcu_sell_plan_stats(dcu_spai_ctx* ctx, long long* slots, long long* uniform_slots);
+
 /* ---- MatrixMarket input (command-line driver) --------------------------------- */
 
 /* Read a MatrixMarket file into host CSC arrays with the semantics of

@@ -158,3 +158,20 @@ def test_host_path_matches_device_path(ctx):
     hx, hm = pin(x0), pin(np.zeros(A.nnz))
     ctx.solve_h_into(A.n, A.nnz, pin(A.ptr), pin(A.idx), pin(A.val), pin(b), hx, mval=hm, precision=N.PREC_M_BF16)
     assert np.array_equal(hx, x_dev) and np.array_equal(hm, m_dev)
+
+
+def test_sell_plan_stats_and_offset_aligned_slices(ctx):
+    """A 3D stencil lays out in offset-uniform slices (no index reads) except
+    where row + offset leaves the matrix; an irregular matrix mostly does not.
+    Both solve to the same iterations as the oracle (the layout only moves
+    zeros around)."""
+    for A, lo, hi in ((W.convdiff3d(16, 20.0), 0.95, 1.0), (W.circuit_like(), 0.0, 0.9)):
+        b, _ = W.rhs_from_solution(A, seed=2)
+        x, _, _, si = ctx.solve_h(A, b, precision=N.PREC_FP64)
+        slots, uni = ctx.sell_plan_stats()
+        assert slots >= A.nnz and 0 <= uni <= slots
+        assert lo <= uni / slots <= hi, (uni, slots)
+        m_o, _, _, _ = oracle.spai(A, "mgs")
+        ref = oracle.bicgstab(A, m_o, b, None, tol=1e-8, tol_mode="rel", maxiter=1000)
+        assert si.status == N.SOLVE_CONVERGED and abs(si.iters - ref["iters"]) <= 1
+        assert np.linalg.norm(b - A.matvec(x)) / np.linalg.norm(b) < 1e-8
