@@ -524,34 +524,54 @@ __global__ void __launch_bounds__(NE_BLOCK) k_spai_ne(NeArgs a) {
     for (int i = 0; i < NE_NJ * (NE_NJ + 1) / 2; ++i) G[i] = T(0);
 #pragma unroll
     for (int j = 0; j < NE_NJ; ++j) g[j] = T(0);
-#pragma unroll
-    for (int ja = 0; ja < NE_NJ; ++ja) {
-      for (int p = cb[ja]; p < cb[ja] + len[ja]; ++p) {
-        const int r = srow[p * NE_BLOCK + tid];
-        const T v = sval[p * NE_BLOCK + tid];
-        if (r == k) g[ja] += v;
-        G[tri(ja, ja)] += v * v;
-      }
-    }
     if (sorted) {
-      // rows ascending in every column: merge each pair of columns
+      // Rows ascending in every column: one K-way merge over the columns.
+      // Each step takes the smallest row r left among the column heads,
+      // forms v = A(r, J) (zero where a column lacks r) and adds v v^T to G
+      // and v to g when r = k.  Every G entry sums its products in ascending
+      // row order, as a pairwise merge would; each entry is read once.  Each
+      // step consumes at least one entry, so it runs at most cand times.
+      int pos[NE_NJ], head[NE_NJ];
 #pragma unroll
-      for (int ja = 0; ja < NE_NJ; ++ja) {
+      for (int j = 0; j < NE_NJ; ++j) {
+        pos[j] = cb[j];
+        head[j] = (len[j] > 0) ? srow[cb[j] * NE_BLOCK + tid] : INT_MAX;
+      }
+      for (int step = 0; step < cand; ++step) {
+        int m = head[0];
 #pragma unroll
-        for (int jb = ja + 1; jb < NE_NJ; ++jb) {
-          int i = cb[ja], j = cb[jb];
-          const int ie = i + len[ja], je = j + len[jb];
-          T acc = T(0);
-          while (i < ie && j < je) {
-            const int ra = srow[i * NE_BLOCK + tid], rb = srow[j * NE_BLOCK + tid];
-            if (ra == rb) acc += sval[i * NE_BLOCK + tid] * sval[j * NE_BLOCK + tid];
-            i += (ra <= rb) ? 1 : 0;
-            j += (rb <= ra) ? 1 : 0;
+        for (int j = 1; j < NE_NJ; ++j) m = min(m, head[j]);
+        if (m == INT_MAX) break;
+        T v[NE_NJ];
+#pragma unroll
+        for (int j = 0; j < NE_NJ; ++j) {
+          v[j] = T(0);
+          if (head[j] == m) {
+            v[j] = sval[pos[j] * NE_BLOCK + tid];
+            ++pos[j];
+            head[j] = (pos[j] < cb[j] + len[j]) ? srow[pos[j] * NE_BLOCK + tid] : INT_MAX;
           }
-          G[tri(ja, jb)] += acc;
+        }
+        if (m == k) {
+#pragma unroll
+          for (int j = 0; j < NE_NJ; ++j) g[j] += v[j];
+        }
+#pragma unroll
+        for (int ja = 0; ja < NE_NJ; ++ja) {
+#pragma unroll
+          for (int jb = ja; jb < NE_NJ; ++jb) G[tri(ja, jb)] += v[ja] * v[jb];
         }
       }
     } else {
+#pragma unroll
+      for (int ja = 0; ja < NE_NJ; ++ja) {
+        for (int p = cb[ja]; p < cb[ja] + len[ja]; ++p) {
+          const int r = srow[p * NE_BLOCK + tid];
+          const T v = sval[p * NE_BLOCK + tid];
+          if (r == k) g[ja] += v;
+          G[tri(ja, ja)] += v * v;
+        }
+      }
 #pragma unroll
       for (int ja = 0; ja < NE_NJ; ++ja) {
         for (int p = cb[ja]; p < cb[ja] + len[ja]; ++p) {
