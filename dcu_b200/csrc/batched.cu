@@ -5,12 +5,13 @@
 // cublas2_pbicgstabv2 (include/bicgstab/bicgstab_solver.h:33-275) with its own
 // rho, alpha, omega, beta and stop test; pairs that converge are frozen (x no
 // longer changes) while the others continue.  Layout: A and M in SELL-32 over
-// all N rows; vectors row-major N x R, so one thread computes its row for all
-// R right-hand sides and every matrix entry read from HBM serves R products
-// (R contiguous doubles per gathered column).  Thread blocks are tiles of 256
-// rows inside one system; each dot product leaves one partial per tile and
-// the last tile of a system to finish sums that system's partials in tile
-// order (deterministic) and updates the system's scalars.
+// all N rows; vectors row-major N x R.  R threads share a row, one per
+// right-hand side, so every matrix entry read from HBM serves R products (a
+// warp broadcast) and a gathered column is R contiguous doubles read by R
+// neighbouring lanes.  Thread blocks are tiles of 256 rows inside one
+// system; each dot product leaves one partial per tile and the last tile of a
+// system to finish sums that system's partials in tile order (deterministic)
+// and updates the system's scalars.
 #include <algorithm>
 
 #include "internal.cuh"
@@ -77,60 +78,97 @@ struct BArgs {
 };
 
 // out[q] = sum_k val * X[col][q], q < R, X row-major with R columns.
-// A slice whose every k has one column offset (su, kd: SellPlan) forms its
+// One SELL-32 row of one right-hand side: sum_k val[q] * xf(col[q]).  A
+// slice whose every k has one column offset (su, kd: SellPlan) forms its
 // columns from the row and reads no index.
-template <int R, typename F>
-__device__ __forceinline__ void sell_row_multi(const long long* __restrict__ off, const int* __restrict__ kd,
-                                               const int* __restrict__ su, const double* __restrict__ val,
-                                               const int* __restrict__ ix, int row, F xf, double (&out)[R]) {
-#pragma unroll
-  for (int q = 0; q < R; ++q) out[q] = 0.0;
+template <typename F>
+__device__ __forceinline__ double sell_row_1(const long long* __restrict__ off, const int* __restrict__ kd,
+                                             const int* __restrict__ su, const double* __restrict__ val,
+                                             const int* __restrict__ ix, int row, F xf) {
   const int sl = row >> 5;
   const long long o0 = __ldg(off + sl), o1 = __ldg(off + sl + 1);
   const long long base = o0 + (row & 31);
   const int w = (int)((o1 - o0) >> 5);
-  const bool uniform = __ldg(su + sl) != 0;
-  const int* __restrict__ kp = kd + (o0 >> 5);
-  for (int k = 0; k < w; ++k) {
-    const long long qk = base + 32ll * k;
-    const double a = __ldcs(val + qk);
-    const int c = uniform ? row + (__ldg(kp + k) >> 1) : __ldcs(ix + qk);
-    double xv[R];
-    xf(c, xv);
+  double acc = 0.0;
+  if (__ldg(su + sl)) {
+    const int* __restrict__ kp = kd + (o0 >> 5);
+    for (int k0 = 0; k0 < w; k0 += 8) {
+      double av[8];
+      int cv[8];
 #pragma unroll
-    for (int q = 0; q < R; ++q) out[q] += a * xv[q];
+      for (int t = 0; t < 8; ++t) {
+        if (k0 + t < w) {
+          av[t] = __ldcs(val + base + 32ll * (k0 + t));
+          cv[t] = row + (__ldg(kp + k0 + t) >> 1);
+        } else {
+          av[t] = 0.0;
+          cv[t] = row;
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < 8; ++t)
+        if (k0 + t < w) acc += av[t] * xf(cv[t]);
+    }
+    return acc;
   }
+  for (int k0 = 0; k0 < w; k0 += 8) {
+    double av[8];
+    int cv[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      if (k0 + t < w) {
+        const long long q = base + 32ll * (k0 + t);
+        av[t] = __ldcs(val + q);
+        cv[t] = __ldcs(ix + q);
+      } else {
+        av[t] = 0.0;
+        cv[t] = row;
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < 8; ++t)
+      if (k0 + t < w) acc += av[t] * xf(cv[t]);
+  }
+  return acc;
 }
 
+// Thread layout: a block covers one tile of BT rows of one system; thread t
+// owns right-hand side q = t % R and takes the tile's rows in R passes of
+// BT / R consecutive rows (row = row0 + pass * BT / R + t / R).  A warp then
+// reads 32 consecutive doubles of each row-major N x R vector, and gathers
+// 32 / R neighbouring rows x R right-hand sides (contiguous) per column
+// offset; each thread carries one right-hand side, so registers stay low.
 template <int R>
-__device__ __forceinline__ void load_row(const double* __restrict__ v, int row, double (&o)[R]) {
-  const double2* p = reinterpret_cast<const double2*>(v + (size_t)row * R);
-#pragma unroll
-  for (int q = 0; q < R / 2; ++q) {
-    const double2 t = __ldg(p + q);
-    o[2 * q] = t.x;
-    o[2 * q + 1] = t.y;
+struct TileRows {
+  int row0, row_end, q, j;
+  __device__ TileRows(const int* tile_row0, const int* sys_off, int tile, int sys) {
+    row0 = tile_row0[tile];
+    row_end = min(row0 + BT, sys_off[sys + 1]);
+    q = threadIdx.x % R;
+    j = threadIdx.x / R;
   }
-  if (R & 1) o[R - 1] = __ldg(v + (size_t)row * R + R - 1);
-}
+  __device__ int row(int pass) const { return row0 + pass * (BT / R) + j; }
+};
 
-// Block sums of ND * R values per thread into part[tile]; the last tile of
-// the system to finish gets the system totals (tile order) in tot and true.
+// Block sums of ND values per thread (thread t adds to right-hand side
+// t % R) into part[tile][d * R + q]; the last tile of the system to finish
+// gets a pointer to the system totals (summed in tile order, entry d * R + q,
+// in shared memory), every other tile nullptr.
 template <int ND, int R>
-__device__ __forceinline__ bool system_reduce(double (&v)[ND][R], double* __restrict__ part, unsigned* cnt, int tile,
-                                              int t0, int t1, int sys, double (&tot)[ND][R]) {
+__device__ __forceinline__ const double* system_reduce(double (&v)[ND], double* __restrict__ part, unsigned* cnt,
+                                                       int tile, int t0, int t1, int sys) {
   __shared__ double red[ND * R][BT_WARPS];
+  __shared__ double totals[ND * R];
   __shared__ int amlast;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
-  for (int d = 0; d < ND; ++d)
+  for (int d = 0; d < ND; ++d) {
+    double xs = v[d];
+    // lanes j * R + q of a warp share q: fold over the row bits
 #pragma unroll
-    for (int q = 0; q < R; ++q) {
-      double xs = v[d][q];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) xs += __shfl_xor_sync(0xffffffffu, xs, o);
-      if (lane == 0) red[d * R + q][wid] = xs;
-    }
+    for (int o = 16; o >= R; o >>= 1) xs += __shfl_xor_sync(0xffffffffu, xs, o);
+    if (lane < R) red[d * R + lane][wid] = xs;
+  }
   __syncthreads();
   if (threadIdx.x < ND * R) {
     double ssum = 0.0;
@@ -145,21 +183,17 @@ __device__ __forceinline__ bool system_reduce(double (&v)[ND][R], double* __rest
     amlast = (done == (unsigned)(t1 - t0 - 1)) ? 1 : 0;
   }
   __syncthreads();
-  if (!amlast) return false;
+  if (!amlast) return nullptr;
   __threadfence();
   // thread j < ND * R sums slot j over the system's tiles in order
   if (threadIdx.x < ND * R) {
     double ssum = 0.0;
     for (int t = t0; t < t1; ++t) ssum += __ldcg(part + (size_t)t * (3 * R) + threadIdx.x);
-    red[threadIdx.x][0] = ssum;
+    totals[threadIdx.x] = ssum;
   }
   __syncthreads();
-#pragma unroll
-  for (int d = 0; d < ND; ++d)
-#pragma unroll
-    for (int q = 0; q < R; ++q) tot[d][q] = red[d * R + q][0];
   if (threadIdx.x == 0) cnt[sys] = 0u;
-  return true;
+  return totals;
 }
 
 __device__ __forceinline__ bool g_finished(const BGlobal* g) { return *(volatile const int*)&g->done != 0; }
@@ -172,36 +206,35 @@ __device__ __forceinline__ bool system_idle(const BArgs<R>& a, int sys) { return
 template <int R>
 __global__ void __launch_bounds__(BT) kb_init(BArgs<R> a, double tol, int tol_mode) {
   const int tile = blockIdx.x, sys = a.tile_sys[tile];
-  const int row = a.tile_row0[tile] + threadIdx.x;
-  const bool valid = row < a.sys_off[sys + 1];
-  double v[3][R] = {};
-  if (valid) {
-    double ax[R], bb[R];
-    sell_row_multi<R>(a.off, a.kd, a.su, a.aval, a.ix, row, [&](int c, double (&o)[R]) { load_row<R>(a.x, c, o); }, ax);
-    load_row<R>(a.b, row, bb);
-#pragma unroll
-    for (int q = 0; q < R; ++q) {
-      const double rr = bb[q] + (-1.0) * ax[q];
-      const size_t i = (size_t)row * R + q;
-      a.r[i] = rr;
-      a.rs[i] = rr;
-      a.p0[i] = 0.0;
-      a.p1[i] = 0.0;
-      a.ay[i] = 0.0;
-      v[0][q] += rr * rr;   // (r*, r) = (r, r) at the start
-      v[1][q] += rr * rr;
-      v[2][q] += bb[q] * bb[q];
-    }
+  const TileRows<R> tr(a.tile_row0, a.sys_off, tile, sys);
+  const int q = tr.q;
+  double v[3] = {0.0, 0.0, 0.0};
+#pragma unroll 1
+  for (int pass = 0; pass < R; ++pass) {
+    const int row = tr.row(pass);
+    if (row >= tr.row_end) break;
+    const double ax = sell_row_1(a.off, a.kd, a.su, a.aval, a.ix, row,
+                                 [&](int c) { return __ldg(a.x + (size_t)c * R + q); });
+    const size_t i = (size_t)row * R + q;
+    const double bb = a.b[i];
+    const double rr = bb + (-1.0) * ax;
+    a.r[i] = rr;
+    a.rs[i] = rr;
+    a.p0[i] = 0.0;
+    a.p1[i] = 0.0;
+    a.ay[i] = 0.0;
+    v[0] += rr * rr;   // (r*, r) = (r, r) at the start
+    v[1] += rr * rr;
+    v[2] += bb * bb;
   }
-  double tot[3][R];
-  if (system_reduce<3, R>(v, a.part, a.cnt, tile, a.tile_off[sys], a.tile_off[sys + 1], sys, tot) &&
-      threadIdx.x == 0) {
+  const double* tot = system_reduce<3, R>(v, a.part, a.cnt, tile, a.tile_off[sys], a.tile_off[sys + 1], sys);
+  if (tot && threadIdx.x == 0) {
     int live = 0;
-    for (int q = 0; q < R; ++q) {
-      const int i = sys * R + q;
-      a.st.rho[i] = tot[0][q];
-      a.st.res[i] = sqrt(tot[1][q]);
-      a.st.bnorm[i] = sqrt(tot[2][q]);
+    for (int qq = 0; qq < R; ++qq) {
+      const int i = sys * R + qq;
+      a.st.rho[i] = tot[0 * R + qq];
+      a.st.res[i] = sqrt(tot[1 * R + qq]);
+      a.st.bnorm[i] = sqrt(tot[2 * R + qq]);
       a.st.thr[i] = (tol_mode == DCU_TOL_REL) ? tol * a.st.bnorm[i] : tol;
       a.st.alpha[i] = 0.0;
       a.st.omega[i] = 1.0;
@@ -223,32 +256,26 @@ __global__ void __launch_bounds__(BT) kb_py(BArgs<R> a) {
   if (g_finished(a.g)) return;
   const int tile = blockIdx.x, sys = a.tile_sys[tile];
   if (system_idle(a, sys)) return;
-  const int row = a.tile_row0[tile] + threadIdx.x;
-  if (row >= a.sys_off[sys + 1]) return;
-  double beta[R], omega[R];
-#pragma unroll
-  for (int q = 0; q < R; ++q) {
-    beta[q] = a.st.beta[sys * R + q];
-    omega[q] = a.st.omega[sys * R + q];
-  }
+  const TileRows<R> tr(a.tile_row0, a.sys_off, tile, sys);
+  const int q = tr.q;
+  const double beta = a.st.beta[sys * R + q], omega = a.st.omega[sys * R + q];
   const int pidx = a.g->pidx;
-  const double* pold = pidx ? a.p1 : a.p0;
-  double* pnew = pidx ? a.p0 : a.p1;
-  auto pf = [&](int c, double (&o)[R]) {
-    double rr[R], pp[R], yy[R];
-    load_row<R>(a.r, c, rr);
-    load_row<R>(pold, c, pp);
-    load_row<R>(a.ay, c, yy);
-#pragma unroll
-    for (int q = 0; q < R; ++q) o[q] = rr[q] + beta[q] * (pp[q] - omega[q] * yy[q]);
+  const double* __restrict__ pold = pidx ? a.p1 : a.p0;
+  double* __restrict__ pnew = pidx ? a.p0 : a.p1;
+  const double* __restrict__ rr = a.r;
+  const double* __restrict__ yy = a.ay;
+  auto pf = [&](int c) {
+    const size_t i = (size_t)c * R + q;
+    return __ldg(rr + i) + beta * (__ldg(pold + i) - omega * __ldg(yy + i));
   };
-  double yv[R], pv[R];
-  sell_row_multi<R>(a.off, a.kd, a.su, a.mval, a.ix, row, pf, yv);
-  pf(row, pv);
-#pragma unroll
-  for (int q = 0; q < R; ++q) {
-    pnew[(size_t)row * R + q] = pv[q];
-    a.y[(size_t)row * R + q] = yv[q];
+#pragma unroll 1
+  for (int pass = 0; pass < R; ++pass) {
+    const int row = tr.row(pass);
+    if (row >= tr.row_end) break;
+    const double yv = sell_row_1(a.off, a.kd, a.su, a.mval, a.ix, row, pf);
+    const size_t i = (size_t)row * R + q;
+    pnew[i] = pf(row);
+    a.y[i] = yv;
   }
 }
 
@@ -258,27 +285,28 @@ __global__ void __launch_bounds__(BT) kb_ay(BArgs<R> a) {
   if (g_finished(a.g)) return;
   const int tile = blockIdx.x, sys = a.tile_sys[tile];
   if (system_idle(a, sys)) return;
-  const int row = a.tile_row0[tile] + threadIdx.x;
-  double v[1][R] = {};
-  if (row < a.sys_off[sys + 1]) {
-    double ayv[R], rsv[R];
-    sell_row_multi<R>(a.off, a.kd, a.su, a.aval, a.ix, row, [&](int c, double (&o)[R]) { load_row<R>(a.y, c, o); }, ayv);
-    load_row<R>(a.rs, row, rsv);
-#pragma unroll
-    for (int q = 0; q < R; ++q) {
-      a.ay[(size_t)row * R + q] = ayv[q];
-      v[0][q] += rsv[q] * ayv[q];
-    }
+  const TileRows<R> tr(a.tile_row0, a.sys_off, tile, sys);
+  const int q = tr.q;
+  const double* __restrict__ y = a.y;
+  double v[1] = {0.0};
+#pragma unroll 1
+  for (int pass = 0; pass < R; ++pass) {
+    const int row = tr.row(pass);
+    if (row >= tr.row_end) break;
+    const double ayv = sell_row_1(a.off, a.kd, a.su, a.aval, a.ix, row,
+                                  [&](int c) { return __ldg(y + (size_t)c * R + q); });
+    const size_t i = (size_t)row * R + q;
+    a.ay[i] = ayv;
+    v[0] += a.rs[i] * ayv;
   }
-  double tot[1][R];
-  if (system_reduce<1, R>(v, a.part, a.cnt, tile, a.tile_off[sys], a.tile_off[sys + 1], sys, tot) &&
-      threadIdx.x == 0) {
-    for (int q = 0; q < R; ++q) {
-      const int i = sys * R + q;
+  const double* tot = system_reduce<1, R>(v, a.part, a.cnt, tile, a.tile_off[sys], a.tile_off[sys + 1], sys);
+  if (tot && threadIdx.x == 0) {
+    for (int qq = 0; qq < R; ++qq) {
+      const int i = sys * R + qq;
       if (!a.st.active[i]) continue;
-      const double alpha = a.st.rho[i] / tot[0][q];
+      const double alpha = a.st.rho[i] / tot[0 * R + qq];
       a.st.alpha[i] = alpha;
-      if (tot[0][q] == 0.0 || !isfinite(alpha)) {
+      if (tot[0 * R + qq] == 0.0 || !isfinite(alpha)) {
         a.st.active[i] = 0;
         a.st.status[i] = DCU_SOLVE_BREAKDOWN;
         a.st.alpha[i] = a.st.omega[i] = a.st.beta[i] = 0.0;
@@ -295,25 +323,23 @@ __global__ void __launch_bounds__(BT) kb_sz(BArgs<R> a) {
   if (g_finished(a.g)) return;
   const int tile = blockIdx.x, sys = a.tile_sys[tile];
   if (system_idle(a, sys)) return;
-  const int row = a.tile_row0[tile] + threadIdx.x;
-  if (row >= a.sys_off[sys + 1]) return;
-  double nalpha[R];
-#pragma unroll
-  for (int q = 0; q < R; ++q) nalpha[q] = -1.0 * a.st.alpha[sys * R + q];
-  auto sf = [&](int c, double (&o)[R]) {
-    double rr[R], yy[R];
-    load_row<R>(a.r, c, rr);
-    load_row<R>(a.ay, c, yy);
-#pragma unroll
-    for (int q = 0; q < R; ++q) o[q] = rr[q] + nalpha[q] * yy[q];
+  const TileRows<R> tr(a.tile_row0, a.sys_off, tile, sys);
+  const int q = tr.q;
+  const double nalpha = -1.0 * a.st.alpha[sys * R + q];
+  const double* __restrict__ rr = a.r;
+  const double* __restrict__ yy = a.ay;
+  auto sf = [&](int c) {
+    const size_t i = (size_t)c * R + q;
+    return __ldg(rr + i) + nalpha * __ldg(yy + i);
   };
-  double zv[R], sv[R];
-  sell_row_multi<R>(a.off, a.kd, a.su, a.mval, a.ix, row, sf, zv);
-  sf(row, sv);
-#pragma unroll
-  for (int q = 0; q < R; ++q) {
-    a.s[(size_t)row * R + q] = sv[q];
-    a.z[(size_t)row * R + q] = zv[q];
+#pragma unroll 1
+  for (int pass = 0; pass < R; ++pass) {
+    const int row = tr.row(pass);
+    if (row >= tr.row_end) break;
+    const double zv = sell_row_1(a.off, a.kd, a.su, a.mval, a.ix, row, sf);
+    const size_t i = (size_t)row * R + q;
+    a.s[i] = sf(row);
+    a.z[i] = zv;
   }
 }
 
@@ -323,28 +349,29 @@ __global__ void __launch_bounds__(BT) kb_az(BArgs<R> a) {
   if (g_finished(a.g)) return;
   const int tile = blockIdx.x, sys = a.tile_sys[tile];
   if (system_idle(a, sys)) return;
-  const int row = a.tile_row0[tile] + threadIdx.x;
-  double v[2][R] = {};
-  if (row < a.sys_off[sys + 1]) {
-    double azv[R], sv[R];
-    sell_row_multi<R>(a.off, a.kd, a.su, a.aval, a.ix, row, [&](int c, double (&o)[R]) { load_row<R>(a.z, c, o); }, azv);
-    load_row<R>(a.s, row, sv);
-#pragma unroll
-    for (int q = 0; q < R; ++q) {
-      a.az[(size_t)row * R + q] = azv[q];
-      v[0][q] += azv[q] * sv[q];
-      v[1][q] += azv[q] * azv[q];
-    }
+  const TileRows<R> tr(a.tile_row0, a.sys_off, tile, sys);
+  const int q = tr.q;
+  const double* __restrict__ z = a.z;
+  double v[2] = {0.0, 0.0};
+#pragma unroll 1
+  for (int pass = 0; pass < R; ++pass) {
+    const int row = tr.row(pass);
+    if (row >= tr.row_end) break;
+    const double azv = sell_row_1(a.off, a.kd, a.su, a.aval, a.ix, row,
+                                  [&](int c) { return __ldg(z + (size_t)c * R + q); });
+    const size_t i = (size_t)row * R + q;
+    a.az[i] = azv;
+    v[0] += azv * a.s[i];
+    v[1] += azv * azv;
   }
-  double tot[2][R];
-  if (system_reduce<2, R>(v, a.part, a.cnt, tile, a.tile_off[sys], a.tile_off[sys + 1], sys, tot) &&
-      threadIdx.x == 0) {
-    for (int q = 0; q < R; ++q) {
-      const int i = sys * R + q;
+  const double* tot = system_reduce<2, R>(v, a.part, a.cnt, tile, a.tile_off[sys], a.tile_off[sys + 1], sys);
+  if (tot && threadIdx.x == 0) {
+    for (int qq = 0; qq < R; ++qq) {
+      const int i = sys * R + qq;
       if (!a.st.active[i]) continue;
-      const double omega = tot[0][q] / tot[1][q];
+      const double omega = tot[0 * R + qq] / tot[1 * R + qq];
       a.st.omega[i] = omega;
-      if (tot[1][q] == 0.0 || omega == 0.0 || !isfinite(omega)) {
+      if (tot[1 * R + qq] == 0.0 || omega == 0.0 || !isfinite(omega)) {
         a.st.active[i] = 0;
         a.st.status[i] = DCU_SOLVE_BREAKDOWN;
         a.st.alpha[i] = a.st.omega[i] = a.st.beta[i] = 0.0;
@@ -361,43 +388,39 @@ __global__ void __launch_bounds__(BT) kb_xr(BArgs<R> a) {
   if (g_finished(a.g)) return;
   const int tile = blockIdx.x, sys = a.tile_sys[tile];
   if (system_idle(a, sys)) return;
-  const int row = a.tile_row0[tile] + threadIdx.x;
-  double v[2][R] = {};
-  if (row < a.sys_off[sys + 1]) {
-    double yv[R], zv[R], sv[R], azv[R], rsv[R], xv[R];
-    load_row<R>(a.y, row, yv);
-    load_row<R>(a.z, row, zv);
-    load_row<R>(a.s, row, sv);
-    load_row<R>(a.az, row, azv);
-    load_row<R>(a.rs, row, rsv);
-    load_row<R>(a.x, row, xv);
-#pragma unroll
-    for (int q = 0; q < R; ++q) {
-      const int i = sys * R + q;
-      const double alpha = a.st.alpha[i], omega = a.st.omega[i];
-      if (a.st.active[i]) {
-        double t = xv[q] + alpha * yv[q];
-        t = t + omega * zv[q];
-        a.x[(size_t)row * R + q] = t;
-      }
-      const double rn = sv[q] + (-1.0 * omega) * azv[q];
-      a.r[(size_t)row * R + q] = rn;
-      v[0][q] += rsv[q] * rn;
-      v[1][q] += rn * rn;
+  const TileRows<R> tr(a.tile_row0, a.sys_off, tile, sys);
+  const int q = tr.q;
+  const int ip = sys * R + q;
+  const double alpha = a.st.alpha[ip], omega = a.st.omega[ip], nomega = -1.0 * omega;
+  const bool active = a.st.active[ip] != 0;
+  double v[2] = {0.0, 0.0};
+#pragma unroll 1
+  for (int pass = 0; pass < R; ++pass) {
+    const int row = tr.row(pass);
+    if (row >= tr.row_end) break;
+    const size_t i = (size_t)row * R + q;
+    const double xv = a.x[i], yv = a.y[i], zv = a.z[i], sv = a.s[i], azv = a.az[i], rsv = a.rs[i];
+    if (active) {
+      double t = xv + alpha * yv;
+      t = t + omega * zv;
+      a.x[i] = t;
     }
+    const double rn = sv + nomega * azv;
+    a.r[i] = rn;
+    v[0] += rsv * rn;
+    v[1] += rn * rn;
   }
-  double tot[2][R];
-  if (system_reduce<2, R>(v, a.part, a.cnt, tile, a.tile_off[sys], a.tile_off[sys + 1], sys, tot) &&
-      threadIdx.x == 0) {
+  const double* tot = system_reduce<2, R>(v, a.part, a.cnt, tile, a.tile_off[sys], a.tile_off[sys + 1], sys);
+  if (tot && threadIdx.x == 0) {
     const int it = a.g->it;
-    for (int q = 0; q < R; ++q) {
-      const int i = sys * R + q;
+    for (int qq = 0; qq < R; ++qq) {
+      const int i = sys * R + qq;
       if (!a.st.active[i]) continue;
-      const double rho_new = tot[0][q];
+      const double rho_new = tot[0 * R + qq];
       const double beta = (rho_new / a.st.rho[i]) * (a.st.alpha[i] / a.st.omega[i]);
       a.st.rho[i] = rho_new;
       a.st.beta[i] = beta;
-      a.st.res[i] = sqrt(tot[1][q]);
+      a.st.res[i] = sqrt(tot[1 * R + qq]);
       a.st.conv_it[i] = it;
       if (!isfinite(a.st.res[i]) || !isfinite(beta) || rho_new == 0.0) {
         a.st.active[i] = 0;
