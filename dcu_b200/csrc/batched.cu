@@ -78,18 +78,62 @@ struct BArgs {
 };
 
 // out[q] = sum_k val * X[col][q], q < R, X row-major with R columns.
-// One SELL-32 row of one right-hand side: sum_k val[q] * xf(col[q]).  A
-// slice whose every k has one column offset (su, kd: SellPlan) forms its
+// V right-hand sides per thread: 2 (one 16-byte load per gathered column)
+// when R >= 2, else 1.
+template <int R>
+__host__ __device__ constexpr int vals_per_thread() {
+  return R >= 2 ? 2 : 1;
+}
+
+template <int V>
+__device__ __forceinline__ void ldv(const double* __restrict__ p, double (&o)[V]) {
+  if constexpr (V == 2) {
+    const double2 t = __ldg(reinterpret_cast<const double2*>(p));
+    o[0] = t.x;
+    o[1] = t.y;
+  } else {
+    o[0] = __ldg(p);
+  }
+}
+template <int V>
+__device__ __forceinline__ void ldp(const double* p, double (&o)[V]) {  // plain load (data written this launch)
+  if constexpr (V == 2) {
+    const double2 t = *reinterpret_cast<const double2*>(p);
+    o[0] = t.x;
+    o[1] = t.y;
+  } else {
+    o[0] = *p;
+  }
+}
+template <int V>
+__device__ __forceinline__ void stv(double* p, const double (&o)[V]) {
+  if constexpr (V == 2) *reinterpret_cast<double2*>(p) = make_double2(o[0], o[1]);
+  else *p = o[0];
+}
+
+// One SELL-32 row for V right-hand sides: acc[e] = sum_k val[q] * xf(col[q])[e].
+// A slice whose every k has one column offset (su, kd: SellPlan) forms its
 // columns from the row and reads no index.
-template <typename F>
-__device__ __forceinline__ double sell_row_1(const long long* __restrict__ off, const int* __restrict__ kd,
-                                             const int* __restrict__ su, const double* __restrict__ val,
-                                             const int* __restrict__ ix, int row, F xf) {
+template <int V, typename F>
+__device__ __forceinline__ void sell_row_v(const long long* __restrict__ off, const int* __restrict__ kd,
+                                           const int* __restrict__ su, const double* __restrict__ val,
+                                           const int* __restrict__ ix, int row, F xf, double (&acc)[V]) {
   const int sl = row >> 5;
   const long long o0 = __ldg(off + sl), o1 = __ldg(off + sl + 1);
   const long long base = o0 + (row & 31);
   const int w = (int)((o1 - o0) >> 5);
-  double acc = 0.0;
+#pragma unroll
+  for (int e = 0; e < V; ++e) acc[e] = 0.0;
+  auto step = [&](const double (&av)[8], const int (&cv)[8], int k0) {
+#pragma unroll
+    for (int t = 0; t < 8; ++t)
+      if (k0 + t < w) {
+        double xv[V];
+        xf(cv[t], xv);
+#pragma unroll
+        for (int e = 0; e < V; ++e) acc[e] += av[t] * xv[e];
+      }
+  };
   if (__ldg(su + sl)) {
     const int* __restrict__ kp = kd + (o0 >> 5);
     for (int k0 = 0; k0 < w; k0 += 8) {
@@ -97,78 +141,69 @@ __device__ __forceinline__ double sell_row_1(const long long* __restrict__ off, 
       int cv[8];
 #pragma unroll
       for (int t = 0; t < 8; ++t) {
-        if (k0 + t < w) {
-          av[t] = __ldcs(val + base + 32ll * (k0 + t));
-          cv[t] = row + (__ldg(kp + k0 + t) >> 1);
-        } else {
-          av[t] = 0.0;
-          cv[t] = row;
-        }
+        av[t] = (k0 + t < w) ? __ldcs(val + base + 32ll * (k0 + t)) : 0.0;
+        cv[t] = (k0 + t < w) ? row + (__ldg(kp + k0 + t) >> 1) : row;
       }
-#pragma unroll
-      for (int t = 0; t < 8; ++t)
-        if (k0 + t < w) acc += av[t] * xf(cv[t]);
+      step(av, cv, k0);
     }
-    return acc;
+    return;
   }
   for (int k0 = 0; k0 < w; k0 += 8) {
     double av[8];
     int cv[8];
 #pragma unroll
     for (int t = 0; t < 8; ++t) {
-      if (k0 + t < w) {
-        const long long q = base + 32ll * (k0 + t);
-        av[t] = __ldcs(val + q);
-        cv[t] = __ldcs(ix + q);
-      } else {
-        av[t] = 0.0;
-        cv[t] = row;
-      }
+      const long long q = base + 32ll * (k0 + t);
+      av[t] = (k0 + t < w) ? __ldcs(val + q) : 0.0;
+      cv[t] = (k0 + t < w) ? __ldcs(ix + q) : row;
     }
-#pragma unroll
-    for (int t = 0; t < 8; ++t)
-      if (k0 + t < w) acc += av[t] * xf(cv[t]);
+    step(av, cv, k0);
   }
-  return acc;
 }
 
-// Thread layout: a block covers one tile of BT rows of one system; thread t
-// owns right-hand side q = t % R and takes the tile's rows in R passes of
-// BT / R consecutive rows (row = row0 + pass * BT / R + t / R).  A warp then
-// reads 32 consecutive doubles of each row-major N x R vector, and gathers
-// 32 / R neighbouring rows x R right-hand sides (contiguous) per column
-// offset; each thread carries one right-hand side, so registers stay low.
+// Thread layout: a block covers one tile of BT rows of one system.  T = R / V
+// threads share a row; thread t owns right-hand sides q0 .. q0 + V - 1 with
+// q0 = (t % T) * V and takes the tile's rows in T passes of BT / T
+// consecutive rows (row = row0 + pass * BT / T + t / T).  A warp reads 32 x V
+// consecutive doubles of each row-major N x R vector and gathers 32 / T
+// neighbouring rows x R right-hand sides (contiguous) per column offset.
 template <int R>
 struct TileRows {
-  int row0, row_end, q, j;
+  static constexpr int V = vals_per_thread<R>();
+  static constexpr int T = R / V;
+  int row0, row_end, q0, j;
   __device__ TileRows(const int* tile_row0, const int* sys_off, int tile, int sys) {
     row0 = tile_row0[tile];
     row_end = min(row0 + BT, sys_off[sys + 1]);
-    q = threadIdx.x % R;
-    j = threadIdx.x / R;
+    q0 = (threadIdx.x % T) * V;
+    j = threadIdx.x / T;
   }
-  __device__ int row(int pass) const { return row0 + pass * (BT / R) + j; }
+  __device__ int row(int pass) const { return row0 + pass * (BT / T) + j; }
 };
 
-// Block sums of ND values per thread (thread t adds to right-hand side
-// t % R) into part[tile][d * R + q]; the last tile of the system to finish
-// gets a pointer to the system totals (summed in tile order, entry d * R + q,
-// in shared memory), every other tile nullptr.
+// Block sums of ND x V values per thread (value [d][e] belongs to right-hand
+// side q0 + e) into part[tile][d * R + q]; the last tile of the system to
+// finish gets a pointer to the system totals (summed in tile order, entry
+// d * R + q, in shared memory), every other tile nullptr.
 template <int ND, int R>
-__device__ __forceinline__ const double* system_reduce(double (&v)[ND], double* __restrict__ part, unsigned* cnt,
-                                                       int tile, int t0, int t1, int sys) {
+__device__ __forceinline__ const double* system_reduce(double (&v)[ND][vals_per_thread<R>()],
+                                                       double* __restrict__ part, unsigned* cnt, int tile, int t0,
+                                                       int t1, int sys) {
+  constexpr int V = vals_per_thread<R>(), T = R / V;
   __shared__ double red[ND * R][BT_WARPS];
   __shared__ double totals[ND * R];
   __shared__ int amlast;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
-  for (int d = 0; d < ND; ++d) {
-    double xs = v[d];
-    // lanes j * R + q of a warp share q: fold over the row bits
+  for (int d = 0; d < ND; ++d)
 #pragma unroll
-    for (int o = 16; o >= R; o >>= 1) xs += __shfl_xor_sync(0xffffffffu, xs, o);
-    if (lane < R) red[d * R + lane][wid] = xs;
-  }
+    for (int e = 0; e < V; ++e) {
+      double xs = v[d][e];
+      // lanes j * T + qt of a warp share qt: fold over the row bits
+#pragma unroll
+      for (int o = 16; o >= T; o >>= 1) xs += __shfl_xor_sync(0xffffffffu, xs, o);
+      if (lane < T) red[d * R + lane * V + e][wid] = xs;
+    }
   __syncthreads();
   if (threadIdx.x < ND * R) {
     double ssum = 0.0;
@@ -205,27 +240,32 @@ __device__ __forceinline__ bool system_idle(const BArgs<R>& a, int sys) { return
 
 template <int R>
 __global__ void __launch_bounds__(BT) kb_init(BArgs<R> a, double tol, int tol_mode) {
+  constexpr int V = vals_per_thread<R>(), T = R / V;
   const int tile = blockIdx.x, sys = a.tile_sys[tile];
   const TileRows<R> tr(a.tile_row0, a.sys_off, tile, sys);
-  const int q = tr.q;
-  double v[3] = {0.0, 0.0, 0.0};
+  double v[3][V] = {};
 #pragma unroll 1
-  for (int pass = 0; pass < R; ++pass) {
+  for (int pass = 0; pass < T; ++pass) {
     const int row = tr.row(pass);
     if (row >= tr.row_end) break;
-    const double ax = sell_row_1(a.off, a.kd, a.su, a.aval, a.ix, row,
-                                 [&](int c) { return __ldg(a.x + (size_t)c * R + q); });
-    const size_t i = (size_t)row * R + q;
-    const double bb = a.b[i];
-    const double rr = bb + (-1.0) * ax;
-    a.r[i] = rr;
-    a.rs[i] = rr;
-    a.p0[i] = 0.0;
-    a.p1[i] = 0.0;
-    a.ay[i] = 0.0;
-    v[0] += rr * rr;   // (r*, r) = (r, r) at the start
-    v[1] += rr * rr;
-    v[2] += bb * bb;
+    double ax[V], bb[V], rr[V], zero[V];
+    sell_row_v<V>(a.off, a.kd, a.su, a.aval, a.ix, row,
+                  [&](int c, double (&o)[V]) { ldv<V>(a.x + (size_t)c * R + tr.q0, o); }, ax);
+    const size_t i = (size_t)row * R + tr.q0;
+    ldv<V>(a.b + i, bb);
+#pragma unroll
+    for (int e = 0; e < V; ++e) {
+      rr[e] = bb[e] + (-1.0) * ax[e];
+      zero[e] = 0.0;
+      v[0][e] += rr[e] * rr[e];   // (r*, r) = (r, r) at the start
+      v[1][e] += rr[e] * rr[e];
+      v[2][e] += bb[e] * bb[e];
+    }
+    stv<V>(a.r + i, rr);
+    stv<V>(a.rs + i, rr);
+    stv<V>(a.p0 + i, zero);
+    stv<V>(a.p1 + i, zero);
+    stv<V>(a.ay + i, zero);
   }
   const double* tot = system_reduce<3, R>(v, a.part, a.cnt, tile, a.tile_off[sys], a.tile_off[sys + 1], sys);
   if (tot && threadIdx.x == 0) {
@@ -253,51 +293,63 @@ __global__ void __launch_bounds__(BT) kb_init(BArgs<R> a, double tol, int tol_mo
 // K1: p = r + beta (p - omega ay) at gathered columns; y = M p
 template <int R>
 __global__ void __launch_bounds__(BT) kb_py(BArgs<R> a) {
+  constexpr int V = vals_per_thread<R>(), T = R / V;
   if (g_finished(a.g)) return;
   const int tile = blockIdx.x, sys = a.tile_sys[tile];
   if (system_idle(a, sys)) return;
   const TileRows<R> tr(a.tile_row0, a.sys_off, tile, sys);
-  const int q = tr.q;
-  const double beta = a.st.beta[sys * R + q], omega = a.st.omega[sys * R + q];
+  double beta[V], omega[V];
+#pragma unroll
+  for (int e = 0; e < V; ++e) {
+    beta[e] = a.st.beta[sys * R + tr.q0 + e];
+    omega[e] = a.st.omega[sys * R + tr.q0 + e];
+  }
   const int pidx = a.g->pidx;
   const double* __restrict__ pold = pidx ? a.p1 : a.p0;
   double* __restrict__ pnew = pidx ? a.p0 : a.p1;
-  const double* __restrict__ rr = a.r;
-  const double* __restrict__ yy = a.ay;
-  auto pf = [&](int c) {
-    const size_t i = (size_t)c * R + q;
-    return __ldg(rr + i) + beta * (__ldg(pold + i) - omega * __ldg(yy + i));
+  auto pf = [&](int c, double (&o)[V]) {
+    const size_t i = (size_t)c * R + tr.q0;
+    double rr[V], pp[V], yy[V];
+    ldv<V>(a.r + i, rr);
+    ldv<V>(pold + i, pp);
+    ldv<V>(a.ay + i, yy);
+#pragma unroll
+    for (int e = 0; e < V; ++e) o[e] = rr[e] + beta[e] * (pp[e] - omega[e] * yy[e]);
   };
 #pragma unroll 1
-  for (int pass = 0; pass < R; ++pass) {
+  for (int pass = 0; pass < T; ++pass) {
     const int row = tr.row(pass);
     if (row >= tr.row_end) break;
-    const double yv = sell_row_1(a.off, a.kd, a.su, a.mval, a.ix, row, pf);
-    const size_t i = (size_t)row * R + q;
-    pnew[i] = pf(row);
-    a.y[i] = yv;
+    double yv[V], pv[V];
+    sell_row_v<V>(a.off, a.kd, a.su, a.mval, a.ix, row, pf, yv);
+    pf(row, pv);
+    const size_t i = (size_t)row * R + tr.q0;
+    stv<V>(pnew + i, pv);
+    stv<V>(a.y + i, yv);
   }
 }
 
 // K2: ay = A y; alpha = rho / (r*, ay)
 template <int R>
 __global__ void __launch_bounds__(BT) kb_ay(BArgs<R> a) {
+  constexpr int V = vals_per_thread<R>(), T = R / V;
   if (g_finished(a.g)) return;
   const int tile = blockIdx.x, sys = a.tile_sys[tile];
   if (system_idle(a, sys)) return;
   const TileRows<R> tr(a.tile_row0, a.sys_off, tile, sys);
-  const int q = tr.q;
-  const double* __restrict__ y = a.y;
-  double v[1] = {0.0};
+  double v[1][V] = {};
 #pragma unroll 1
-  for (int pass = 0; pass < R; ++pass) {
+  for (int pass = 0; pass < T; ++pass) {
     const int row = tr.row(pass);
     if (row >= tr.row_end) break;
-    const double ayv = sell_row_1(a.off, a.kd, a.su, a.aval, a.ix, row,
-                                  [&](int c) { return __ldg(y + (size_t)c * R + q); });
-    const size_t i = (size_t)row * R + q;
-    a.ay[i] = ayv;
-    v[0] += a.rs[i] * ayv;
+    double ayv[V], rsv[V];
+    sell_row_v<V>(a.off, a.kd, a.su, a.aval, a.ix, row,
+                  [&](int c, double (&o)[V]) { ldv<V>(a.y + (size_t)c * R + tr.q0, o); }, ayv);
+    const size_t i = (size_t)row * R + tr.q0;
+    ldv<V>(a.rs + i, rsv);
+    stv<V>(a.ay + i, ayv);
+#pragma unroll
+    for (int e = 0; e < V; ++e) v[0][e] += rsv[e] * ayv[e];
   }
   const double* tot = system_reduce<1, R>(v, a.part, a.cnt, tile, a.tile_off[sys], a.tile_off[sys + 1], sys);
   if (tot && threadIdx.x == 0) {
@@ -320,49 +372,59 @@ __global__ void __launch_bounds__(BT) kb_ay(BArgs<R> a) {
 // K3: s = r - alpha ay (on the fly at gathered columns); z = M s
 template <int R>
 __global__ void __launch_bounds__(BT) kb_sz(BArgs<R> a) {
+  constexpr int V = vals_per_thread<R>(), T = R / V;
   if (g_finished(a.g)) return;
   const int tile = blockIdx.x, sys = a.tile_sys[tile];
   if (system_idle(a, sys)) return;
   const TileRows<R> tr(a.tile_row0, a.sys_off, tile, sys);
-  const int q = tr.q;
-  const double nalpha = -1.0 * a.st.alpha[sys * R + q];
-  const double* __restrict__ rr = a.r;
-  const double* __restrict__ yy = a.ay;
-  auto sf = [&](int c) {
-    const size_t i = (size_t)c * R + q;
-    return __ldg(rr + i) + nalpha * __ldg(yy + i);
+  double nalpha[V];
+#pragma unroll
+  for (int e = 0; e < V; ++e) nalpha[e] = -1.0 * a.st.alpha[sys * R + tr.q0 + e];
+  auto sf = [&](int c, double (&o)[V]) {
+    const size_t i = (size_t)c * R + tr.q0;
+    double rr[V], yy[V];
+    ldv<V>(a.r + i, rr);
+    ldv<V>(a.ay + i, yy);
+#pragma unroll
+    for (int e = 0; e < V; ++e) o[e] = rr[e] + nalpha[e] * yy[e];
   };
 #pragma unroll 1
-  for (int pass = 0; pass < R; ++pass) {
+  for (int pass = 0; pass < T; ++pass) {
     const int row = tr.row(pass);
     if (row >= tr.row_end) break;
-    const double zv = sell_row_1(a.off, a.kd, a.su, a.mval, a.ix, row, sf);
-    const size_t i = (size_t)row * R + q;
-    a.s[i] = sf(row);
-    a.z[i] = zv;
+    double zv[V], sv[V];
+    sell_row_v<V>(a.off, a.kd, a.su, a.mval, a.ix, row, sf, zv);
+    sf(row, sv);
+    const size_t i = (size_t)row * R + tr.q0;
+    stv<V>(a.s + i, sv);
+    stv<V>(a.z + i, zv);
   }
 }
 
 // K4: az = A z; omega = (az, s) / (az, az)
 template <int R>
 __global__ void __launch_bounds__(BT) kb_az(BArgs<R> a) {
+  constexpr int V = vals_per_thread<R>(), T = R / V;
   if (g_finished(a.g)) return;
   const int tile = blockIdx.x, sys = a.tile_sys[tile];
   if (system_idle(a, sys)) return;
   const TileRows<R> tr(a.tile_row0, a.sys_off, tile, sys);
-  const int q = tr.q;
-  const double* __restrict__ z = a.z;
-  double v[2] = {0.0, 0.0};
+  double v[2][V] = {};
 #pragma unroll 1
-  for (int pass = 0; pass < R; ++pass) {
+  for (int pass = 0; pass < T; ++pass) {
     const int row = tr.row(pass);
     if (row >= tr.row_end) break;
-    const double azv = sell_row_1(a.off, a.kd, a.su, a.aval, a.ix, row,
-                                  [&](int c) { return __ldg(z + (size_t)c * R + q); });
-    const size_t i = (size_t)row * R + q;
-    a.az[i] = azv;
-    v[0] += azv * a.s[i];
-    v[1] += azv * azv;
+    double azv[V], sv[V];
+    sell_row_v<V>(a.off, a.kd, a.su, a.aval, a.ix, row,
+                  [&](int c, double (&o)[V]) { ldv<V>(a.z + (size_t)c * R + tr.q0, o); }, azv);
+    const size_t i = (size_t)row * R + tr.q0;
+    ldv<V>(a.s + i, sv);
+    stv<V>(a.az + i, azv);
+#pragma unroll
+    for (int e = 0; e < V; ++e) {
+      v[0][e] += azv[e] * sv[e];
+      v[1][e] += azv[e] * azv[e];
+    }
   }
   const double* tot = system_reduce<2, R>(v, a.part, a.cnt, tile, a.tile_off[sys], a.tile_off[sys + 1], sys);
   if (tot && threadIdx.x == 0) {
@@ -385,30 +447,45 @@ __global__ void __launch_bounds__(BT) kb_az(BArgs<R> a) {
 // K5: x += alpha y + omega z (active pairs); r = s - omega az; rho, beta, ||r||
 template <int R>
 __global__ void __launch_bounds__(BT) kb_xr(BArgs<R> a) {
+  constexpr int V = vals_per_thread<R>(), T = R / V;
   if (g_finished(a.g)) return;
   const int tile = blockIdx.x, sys = a.tile_sys[tile];
   if (system_idle(a, sys)) return;
   const TileRows<R> tr(a.tile_row0, a.sys_off, tile, sys);
-  const int q = tr.q;
-  const int ip = sys * R + q;
-  const double alpha = a.st.alpha[ip], omega = a.st.omega[ip], nomega = -1.0 * omega;
-  const bool active = a.st.active[ip] != 0;
-  double v[2] = {0.0, 0.0};
+  double alpha[V], omega[V];
+  bool active[V];
+#pragma unroll
+  for (int e = 0; e < V; ++e) {
+    const int ip = sys * R + tr.q0 + e;
+    alpha[e] = a.st.alpha[ip];
+    omega[e] = a.st.omega[ip];
+    active[e] = a.st.active[ip] != 0;
+  }
+  double v[2][V] = {};
 #pragma unroll 1
-  for (int pass = 0; pass < R; ++pass) {
+  for (int pass = 0; pass < T; ++pass) {
     const int row = tr.row(pass);
     if (row >= tr.row_end) break;
-    const size_t i = (size_t)row * R + q;
-    const double xv = a.x[i], yv = a.y[i], zv = a.z[i], sv = a.s[i], azv = a.az[i], rsv = a.rs[i];
-    if (active) {
-      double t = xv + alpha * yv;
-      t = t + omega * zv;
-      a.x[i] = t;
+    const size_t i = (size_t)row * R + tr.q0;
+    double xv[V], yv[V], zv[V], sv[V], azv[V], rsv[V], rn[V];
+    ldp<V>(a.x + i, xv);
+    ldv<V>(a.y + i, yv);
+    ldv<V>(a.z + i, zv);
+    ldv<V>(a.s + i, sv);
+    ldv<V>(a.az + i, azv);
+    ldv<V>(a.rs + i, rsv);
+#pragma unroll
+    for (int e = 0; e < V; ++e) {
+      if (active[e]) {
+        double t = xv[e] + alpha[e] * yv[e];
+        xv[e] = t + omega[e] * zv[e];
+      }
+      rn[e] = sv[e] + (-1.0 * omega[e]) * azv[e];
+      v[0][e] += rsv[e] * rn[e];
+      v[1][e] += rn[e] * rn[e];
     }
-    const double rn = sv + nomega * azv;
-    a.r[i] = rn;
-    v[0] += rsv * rn;
-    v[1] += rn * rn;
+    stv<V>(a.x + i, xv);
+    stv<V>(a.r + i, rn);
   }
   const double* tot = system_reduce<2, R>(v, a.part, a.cnt, tile, a.tile_off[sys], a.tile_off[sys + 1], sys);
   if (tot && threadIdx.x == 0) {
