@@ -268,6 +268,11 @@ def run_extra(args, rank, world):
                     "own iteration count", "bytes": int(total), "solve_ms": round(si.ms, 3),
                     "achieved": round(gbs, 1), "peak": peak, "unit": "GB/s", "frac": round(gbs / peak, 3),
                     "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
+    if args.workload == "grad512":
+        bi, si = ctx.last_solve
+        ai = ctx.last_adjoint
+        cfg.update({"forward_iters": si.iters, "forward_build_ms": round(bi.ms, 3), "forward_solve_ms": round(si.ms, 3),
+                    "adjoint_iters": ai.iters, "adjoint_solve_ms": round(ai.ms, 3)})
     line = {"metric": metric, "value": round(v, 3), "unit": "ms", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(v, 3), "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg}

@@ -156,6 +156,10 @@ class Context:
         self._check(self._L.dcu_profile_iteration_kernels(self.h, reps, ms, 16, C.byref(cnt)))
         return [float(ms[i]) for i in range(cnt.value)]
 
+    def set_iteration_mode(self, mode: int):
+        """N.ITER_AUTO / N.ITER_GRAPH / N.ITER_PERSISTENT (dcu_spai_set_iteration_mode)."""
+        self._check(self._L.dcu_spai_set_iteration_mode(self.h, int(mode)))
+
     def sell_plan_stats(self):
         """(slots, uniform_slots) of the last SELL layout built on this context."""
         s, u = C.c_longlong(), C.c_longlong()
@@ -179,6 +183,7 @@ class Context:
         info = N.SolveInfo()
         self._check(self._L.dcu_bicgstab_transpose_d(self.h, n, nnz, _p(ptr_d), _p(idx_d), _p(val_d), _p(mval_d),
                                                      _p(b_d), _p(x_d), C.byref(o), C.byref(info)))
+        self.last_adjoint = info
         return info
 
     def sampled_outer_d(self, n, nnz, ptr_d, idx_d, u_d, v_d, alpha, out_d):
@@ -204,6 +209,7 @@ class Context:
         bi, si = N.BuildInfo(), N.SolveInfo()
         self._check(self._L.dcu_spai_solve_d(self.h, n, nnz, _p(ptr_d), _p(idx_d), _p(val_d), _p(b_d), _p(x_d),
                                              C.byref(o), _p(mval_d), C.byref(bi), C.byref(si)))
+        self.last_solve = (bi, si)
         return bi, si
 
 
