@@ -156,10 +156,6 @@ class Context:
         self._check(self._L.dcu_profile_iteration_kernels(self.h, reps, ms, 16, C.byref(cnt)))
         return [float(ms[i]) for i in range(cnt.value)]
 
-    def set_iteration_mode(self, mode: int):
-        """N.ITER_AUTO / N.ITER_GRAPH / N.ITER_PERSISTENT (dcu_spai_set_iteration_mode)."""
-        self._check(self._L.dcu_spai_set_iteration_mode(self.h, int(mode)))
-
     def sell_plan_stats(self):
         """(slots, uniform_slots) of the last SELL layout built on this context."""
         s, u = C.c_longlong(), C.c_longlong()

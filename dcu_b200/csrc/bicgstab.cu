@@ -36,8 +36,6 @@ namespace {
 constexpr int BI_BLOCK = 256;
 constexpr int BI_WARPS = BI_BLOCK / 32;
 constexpr int CHUNK_ITERS = 8;  // iterations per graph launch
-// largest system solved by the persistent kernel (its vectors fit in L2)
-constexpr int kPersistMaxN = 1 << 19;
 
 enum { ST_RUN = -1 };
 
@@ -277,7 +275,7 @@ __global__ void __launch_bounds__(BI_BLOCK) k_bi_py(BiArgs<MT, IT, VT> a) {
 // more than the gathers they save, so K1 stays fused there; K3 gathers two
 // vectors and stays fused always.
 template <typename MT>
-__host__ __device__ constexpr bool split_k1() {
+constexpr bool split_k1() {
   return !std::is_same<MT, double>::value;
 }
 
@@ -490,246 +488,6 @@ __global__ void __launch_bounds__(BI_BLOCK) k_bi_true(BiArgs<MT, IT, VT> a, int 
   }
 }
 
-// ---------------------------------------------------------------------------
-// Persistent solver for systems whose iteration is bound by launch and
-// reduction-tail latency rather than bandwidth (the vectors fit in L2).  One
-// cooperative launch (every block resident) runs the iterations; the kernel
-// boundaries become grid barriers and the last-block reductions become
-// "every block sums all block partials in the same order", so every block
-// derives the same alpha, omega, beta and stop decision.  Vectors written
-// inside the launch are read through L2 only (__ldcg): L1 is not coherent
-// across SMs within one launch.  Each thread keeps the same rows in every
-// phase.  The recurrences, stop tests and counter are those of the graph
-// path (K1-K5 above).
-// ---------------------------------------------------------------------------
-struct PSync {
-  unsigned* count;  // arrivals at the current barrier
-  unsigned* gen;    // barrier generation
-  int* err;         // set when a barrier wait gives up
-};
-
-constexpr long long kBarrierSpins = 1ll << 24;  // x 128 ns sleeps: about 2 s
-
-// Grid barrier; false (and *err set) when the wait gave up, which only a
-// logic error can cause since every block is resident.
-__device__ __forceinline__ bool grid_sync(const PSync& ps) {
-  __shared__ int s_fail;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    s_fail = 0;
-    volatile unsigned* vgen = ps.gen;
-    const unsigned g = *vgen;
-    __threadfence();
-    const unsigned arrived = atomicAdd(ps.count, 1u) + 1u;
-    if (arrived == gridDim.x) {
-      atomicExch(ps.count, 0u);
-      __threadfence();
-      atomicAdd(ps.gen, 1u);
-    } else {
-      long long spins = 0;
-      while (*vgen == g) {
-        if (++spins > kBarrierSpins) {
-          atomicExch(ps.err, 1);
-          s_fail = 1;
-          break;
-        }
-        __nanosleep(128);
-      }
-    }
-    __threadfence();
-  }
-  __syncthreads();
-  return s_fail == 0;
-}
-
-// Block sums of ND per-thread values into part[blockIdx.x * 3 + d].
-template <int ND>
-__device__ __forceinline__ void block_partial(double (&v)[ND], double* __restrict__ part) {
-  __shared__ double red[ND][BI_WARPS];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-  for (int d = 0; d < ND; ++d) {
-    double x = v[d];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-    if (lane == 0) red[d][wid] = x;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int d = 0; d < ND; ++d) {
-      double t = 0.0;
-#pragma unroll
-      for (int w = 0; w < BI_WARPS; ++w) t += red[d][w];
-      part[blockIdx.x * 3 + d] = t;
-    }
-  }
-  __syncthreads();
-}
-
-// Totals of the gridDim.x block partials, the same sums in the same order in
-// every block; every thread receives them.
-template <int ND>
-__device__ __forceinline__ void grid_totals(const double* __restrict__ part, double (&tot)[ND]) {
-  __shared__ double red[ND][BI_WARPS];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-  for (int d = 0; d < ND; ++d) {
-    double x = 0.0;
-    for (int i = threadIdx.x; i < (int)gridDim.x; i += BI_BLOCK) x += __ldcg(part + i * 3 + d);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-    if (lane == 0) red[d][wid] = x;
-  }
-  __syncthreads();
-#pragma unroll
-  for (int d = 0; d < ND; ++d) {
-    double t = 0.0;
-#pragma unroll
-    for (int w = 0; w < BI_WARPS; ++w) t += red[d][w];
-    tot[d] = t;
-  }
-  __syncthreads();
-}
-
-template <typename T>
-__device__ __forceinline__ double ldc(const T* p) { return (double)__ldcg(p); }
-__device__ __forceinline__ double ldc(const __nv_bfloat16* p) {
-  const unsigned short u = __ldcg(reinterpret_cast<const unsigned short*>(p));
-  return (double)__uint_as_float((unsigned)u << 16);
-}
-
-template <typename MT, typename IT, typename VT>
-__global__ void __launch_bounds__(BI_BLOCK) k_bi_persist(BiArgs<MT, IT, VT> a, PSync ps) {
-  constexpr bool split = split_k1<MT>();
-  Scal* S = a.S;
-  if (*(volatile const int*)&S->done) return;  // every block reads the same value
-  double rho = S->rho, alpha = S->alpha, omega = S->omega, beta = S->beta, res = S->res;
-  const double thr = S->thr;
-  int it = S->it, pidx = S->pidx;
-  const int maxiter = S->maxiter, verify = S->verify;
-  int status = ST_RUN, verify_pending = 0;
-  const int n = a.n, stride = gridDim.x * BI_BLOCK, t0 = blockIdx.x * BI_BLOCK + threadIdx.x;
-  for (;;) {
-    // K1: p = r + beta (p - omega ay); y = M p
-    if (split) {
-      for (int r = t0; r < n; r += stride)
-        a.p0[r] = (VT)(ldc(a.r + r) + beta * (ldc(a.p0 + r) - omega * ldc(a.ay + r)));
-      if (!grid_sync(ps)) return;
-      for (int r = t0; r < n; r += stride)
-        a.y[r] = (VT)sell_row(a.off, a.kd, a.su, a.mval, a.ix, r, [&](int c) { return ldc(a.p0 + c); });
-    } else {
-      const VT* pold = pidx ? a.p1 : a.p0;
-      VT* pnew = pidx ? a.p0 : a.p1;
-      auto pf = [&](int c) { return ldc(a.r + c) + beta * (ldc(pold + c) - omega * ldc(a.ay + c)); };
-      for (int r = t0; r < n; r += stride) {
-        const double yv = sell_row(a.off, a.kd, a.su, a.mval, a.ix, r, pf);
-        pnew[r] = (VT)pf(r);
-        a.y[r] = (VT)yv;
-      }
-    }
-    if (!grid_sync(ps)) return;
-    // K2: ay = A y; alpha = rho / (r*, ay)
-    {
-      double v[1] = {0.0};
-      for (int r = t0; r < n; r += stride) {
-        const double ayv = sell_row(a.off, a.kd, a.su, a.aval, a.ix, r, [&](int c) { return ldc(a.y + c); });
-        a.ay[r] = ayv;
-        v[0] += (double)__ldg(a.rs + r) * ayv;
-      }
-      block_partial<1>(v, a.part);
-      if (!grid_sync(ps)) return;
-      double tot[1];
-      grid_totals<1>(a.part, tot);
-      alpha = rho / tot[0];
-      if (tot[0] == 0.0 || bad(alpha)) {
-        status = DCU_SOLVE_BREAKDOWN;
-        break;
-      }
-    }
-    // K3: s = r - alpha ay (at gathered columns); z = M s
-    {
-      const double nalpha = -1.0 * alpha;
-      auto sf = [&](int c) { return ldc(a.r + c) + nalpha * ldc(a.ay + c); };
-      for (int r = t0; r < n; r += stride) {
-        const double zv = sell_row(a.off, a.kd, a.su, a.mval, a.ix, r, sf);
-        a.s[r] = ldc(a.r + r) + nalpha * ldc(a.ay + r);
-        a.z[r] = (VT)zv;
-      }
-    }
-    if (!grid_sync(ps)) return;
-    // K4: az = A z; omega = (az, s) / (az, az)
-    {
-      double v[2] = {0.0, 0.0};
-      for (int r = t0; r < n; r += stride) {
-        const double azv = sell_row(a.off, a.kd, a.su, a.aval, a.ix, r, [&](int c) { return ldc(a.z + c); });
-        a.az[r] = azv;
-        v[0] += azv * ldc(a.s + r);
-        v[1] += azv * azv;
-      }
-      block_partial<2>(v, a.part);
-      if (!grid_sync(ps)) return;
-      double tot[2];
-      grid_totals<2>(a.part, tot);
-      omega = tot[0] / tot[1];
-      if (tot[1] == 0.0 || omega == 0.0 || bad(omega)) {
-        status = DCU_SOLVE_BREAKDOWN;
-        break;
-      }
-    }
-    // K5: x += alpha y + omega z; r = s - omega az; rho, beta, ||r||, stop test
-    {
-      const double nomega = -1.0 * omega;
-      double v[2] = {0.0, 0.0};
-      for (int r = t0; r < n; r += stride) {
-        double xv = ldc(a.x + r);
-        xv = xv + alpha * ldc(a.y + r);
-        xv = xv + omega * ldc(a.z + r);
-        a.x[r] = xv;
-        const double rn = ldc(a.s + r) + nomega * ldc(a.az + r);
-        a.r[r] = rn;
-        v[0] += (double)__ldg(a.rs + r) * rn;
-        v[1] += rn * rn;
-      }
-      block_partial<2>(v, a.part);
-      if (!grid_sync(ps)) return;
-      double tot[2];
-      grid_totals<2>(a.part, tot);
-      const double rho_new = tot[0];
-      beta = (rho_new / rho) * (alpha / omega);
-      rho = rho_new;
-      res = sqrt(tot[1]);
-      pidx ^= 1;
-      if (bad(res) || bad(beta) || rho_new == 0.0) {
-        status = DCU_SOLVE_BREAKDOWN;
-        break;
-      }
-      if (res < thr) {
-        if (verify) verify_pending = 1;
-        else status = DCU_SOLVE_CONVERGED;
-        break;
-      }
-      it += 1;
-      if (it >= maxiter) {
-        status = DCU_SOLVE_MAXITER;
-        break;
-      }
-    }
-  }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    S->rho = rho;
-    S->alpha = alpha;
-    S->omega = omega;
-    S->beta = beta;
-    S->res = res;
-    S->it = it;
-    S->pidx = pidx;
-    S->verify_pending = verify_pending;
-    if (!verify_pending) S->status = status;
-    S->done = 1;
-  }
-}
-
 template <typename K, typename A>
 cudaError_t launch_pdl(K kernel, int grid, cudaStream_t st, const A& args) {
   cudaLaunchConfig_t cfg = {};
@@ -767,30 +525,14 @@ int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval,
   const int g_tr = gsize((const void*)k_bi_true<MT, IT, VT>);
   const int g_p = gsize((const void*)k_bi_p<MT, IT, VT>);
   const int g_y = gsize((const void*)k_bi_y<MT, IT, VT>);
-  // Persistent path (one cooperative launch; every block must be resident)
-  // for systems up to kPersistMaxN rows, where launch and reduction latency
-  // bound the iteration; 0 when it cannot be used.
-  int g_ps = 0;
-  if (c->iter_mode == DCU_ITER_PERSISTENT || (c->iter_mode == DCU_ITER_AUTO && n <= kPersistMaxN)) {
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k_bi_persist<MT, IT, VT>, BI_BLOCK, 0) ==
-            cudaSuccess &&
-        per_sm > 0)
-      g_ps = std::min(per_sm * c->sms, std::max(1, (n + BI_BLOCK - 1) / BI_BLOCK));
-    else
-      cudaGetLastError();
-  }
-  const bool persist = g_ps > 0;
-  const int grid = std::max({g_init, g_py, g_ay, g_sz, g_az, g_xr, g_tr, g_p, g_y, g_ps});  // partial-sum slots
+  const int grid = std::max({g_init, g_py, g_ay, g_sz, g_az, g_xr, g_tr, g_p, g_y});  // partial-sum slots
   constexpr bool split = split_k1<MT>();
   // vectors: r, ay, s, az (double) + rs, p0, p1, y, z (VT), 256-byte aligned
   auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
   const size_t nd = al(sizeof(double) * (size_t)n), nv = al(sizeof(VT) * (size_t)n);
   DCU_TRY(ensure(c, B_VEC, 4 * nd + 5 * nv));
   DCU_TRY(ensure(c, B_PART, sizeof(double) * 3 * (size_t)grid + 256));
-  // scalars, then the persistent path's barrier words (count, generation, error)
-  constexpr size_t kSyncOff = (sizeof(Scal) + 63) & ~(size_t)63;
-  DCU_TRY(ensure(c, B_SCAL, kSyncOff + 64));
+  DCU_TRY(ensure(c, B_SCAL, sizeof(Scal)));
   char* base = bp<char>(c, B_VEC);
   BiArgs<MT, IT, VT> a;
   std::memset(&a, 0, sizeof(a));  // padding included: the struct keys the graph cache
@@ -814,10 +556,6 @@ int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval,
   a.z = (VT*)(base + 4 * nd + 4 * nv);
   a.part = bp<double>(c, B_PART);
   a.S = bp<Scal>(c, B_SCAL);
-  PSync ps;
-  ps.count = reinterpret_cast<unsigned*>(bp<char>(c, B_SCAL) + kSyncOff);
-  ps.gen = ps.count + 1;
-  ps.err = reinterpret_cast<int*>(ps.count + 2);
   if (reinterpret_cast<uintptr_t>(x) % 16 != 0)
     return fail(c, DCU_ERR_ARG, "x must be 16-byte aligned (cudaMalloc pointers are)");
   DCU_CUDA(c, cudaMemsetAsync(a.S, 0, sizeof(Scal), c->stream));
@@ -837,7 +575,7 @@ int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval,
   GraphSlot* ge = nullptr;
   for (auto& e : c->graphs)
     if (e.key == key) ge = &e;
-  if (!ge && !persist) {
+  if (!ge) {
     cudaGraph_t g = nullptr;
     DCU_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     cudaError_t le = cudaSuccess;
@@ -905,19 +643,7 @@ int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval,
   const long long max_chunks = (long long)maxiter / CHUNK_ITERS + 4;
   for (int restarts = 0;; ++restarts) {
     if (restarts > maxiter + 1) return fail(c, DCU_ERR_CUDA, "solver did not terminate (restarts)");
-    if (persist) {
-      // runs until the recurrence stops (at most maxiter iterations)
-      DCU_CUDA(c, cudaMemsetAsync(ps.count, 0, 3 * sizeof(unsigned), c->stream));
-      void* args[] = {(void*)&a, (void*)&ps};
-      DCU_CUDA(c, cudaLaunchCooperativeKernel((const void*)k_bi_persist<MT, IT, VT>, dim3(g_ps), dim3(BI_BLOCK), args, 0,
-                                              c->stream));
-      c->launches += 1;
-      int* perr = reinterpret_cast<int*>(reinterpret_cast<char*>(c->pinned) + 2048);
-      DCU_CUDA(c, cudaMemcpyAsync(perr, ps.err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-      DCU_CUDA(c, cudaStreamSynchronize(c->stream));
-      if (*perr) return fail(c, DCU_ERR_CUDA, "persistent solver: a grid barrier wait gave up");
-    }
-    for (long long i = 0; !persist; ++i) {
+    for (long long i = 0;; ++i) {
       if (i > max_chunks) return fail(c, DCU_ERR_CUDA, "solver did not terminate (chunks)");
       DCU_CUDA(c, cudaGraphLaunch(ge->exec, c->stream));
       c->launches += ge->nodes;

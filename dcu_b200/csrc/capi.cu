@@ -475,14 +475,6 @@ int dcu_batch_solve_d(dcu_spai_ctx* c, int nsys, const int* sys_off, int n, int 
   }
 }
 
-int dcu_spai_set_iteration_mode(dcu_spai_ctx* c, int mode) {
-  if (!c) return DCU_ERR_ARG;
-  if (mode < DCU_ITER_AUTO || mode > DCU_ITER_PERSISTENT)
-    return dcu::fail(c, DCU_ERR_ARG, "unknown iteration mode %d", mode);
-  c->iter_mode = mode;
-  return DCU_OK;
-}
-
 int dcu_sell_plan_stats(dcu_spai_ctx* c, long long* slots, long long* uniform_slots) {
   if (!c) return DCU_ERR_ARG;
   StreamScope scope(c);

@@ -83,7 +83,6 @@ struct Ctx {
   size_t smem_optin = 0;
   cudaStream_t stream = nullptr;       // the context's own non-blocking stream
   cudaStream_t copy_stream = nullptr;  // host-API uploads that overlap work on `stream`
-  int iter_mode = 0;                   // dcu_iteration_mode
   cudaStream_t user_stream = nullptr;  // caller's stream to order against (optional)
   cudaEvent_t ev_sync = nullptr;       // ordering between user_stream and stream
   std::string err;

@@ -18,7 +18,6 @@ OK, ERR_ARG, ERR_CUDA, ERR_ALLOC, ERR_NO_DEVICE, ERR_LIMIT = range(6)
 SCHED_BALANCED_COLUMNS, SCHED_BALANCED_NNZ = 0, 1
 # dcu_precision
 PREC_FP64, PREC_MIXED_FP32, PREC_MIXED_BF16, PREC_M_FP32, PREC_M_BF16 = 0, 1, 2, 3, 4
-ITER_AUTO, ITER_GRAPH, ITER_PERSISTENT = 0, 1, 2
 # dcu_ls_method
 LS_AUTO, LS_HOUSEHOLDER, LS_NORMAL_EQ = 0, 1, 2
 # dcu_tol_mode
@@ -75,7 +74,6 @@ SIGNATURES = {
                                C.POINTER(BuildInfo), C.POINTER(SolveInfo)]),
     "dcu_profile_iteration_kernels": (_i, [_vp, _i, C.POINTER(C.c_float), _i, C.POINTER(_i)]),
     "dcu_sell_plan_stats": (_i, [_vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
-    "dcu_spai_set_iteration_mode": (_i, [_vp, _i]),
     "dcu_mtx_read": (_i, [C.c_char_p, C.POINTER(_i), C.POINTER(_i), C.POINTER(C.POINTER(_i)),
                           C.POINTER(C.POINTER(_i)), C.POINTER(C.POINTER(C.c_double))]),
     "dcu_mtx_free": (None, [_vp]),

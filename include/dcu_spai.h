@@ -271,19 +271,6 @@ int dcu_batch_solve_d(dcu_spai_ctx* ctx, int nsys, const int* sys_off, int n, in
  * smaller.  The solver vectors and x are left in an unspecified state. */
 int dcu_profile_iteration_kernels(dcu_spai_ctx* ctx, int reps, float* ms_out, int cap, int* count);
 
-/* How BiCGSTAB (single system, dcu_bicgstab_* / dcu_spai_solve_* and the
- * adjoint) runs its iterations on this context.  AUTO: the persistent kernel
- * for systems up to 2^19 rows (their iteration is bound by launch and
- * reduction latency), else the graph of fused kernels.  GRAPH: CUDA graphs of
- * 8 iterations of the fused kernels, programmatic dependent launch.
- * PERSISTENT: one cooperative launch whose blocks run every iteration,
- * separated by grid barriers (DCU_ERR_CUDA if the device refuses the
- * cooperative launch).  Both follow the same recurrences and stop tests;
- * dot products are summed in a different (fixed) order.  No counterpart in
- * the reference. */
-typedef enum { DCU_ITER_AUTO = 0, DCU_ITER_GRAPH = 1, DCU_ITER_PERSISTENT = 2 } dcu_iteration_mode;
-int dcu_spai_set_iteration_mode(dcu_spai_ctx* ctx, int mode);
-
 /* Diagnostics of the last SELL-32 layout built on this context (by any solve
  * that runs BiCGSTAB): *slots = slots including padding, *uniform_slots =
  * slots in slices whose every entry position has one column offset for all

@@ -175,66 +175,3 @@ def test_sell_plan_stats_and_offset_aligned_slices(ctx):
         ref = oracle.bicgstab(A, m_o, b, None, tol=1e-8, tol_mode="rel", maxiter=1000)
         assert si.status == N.SOLVE_CONVERGED and abs(si.iters - ref["iters"]) <= 1
         assert np.linalg.norm(b - A.matvec(x)) / np.linalg.norm(b) < 1e-8
-
-
-@pytest.fixture
-def mode_ctx(ctx):
-    """The session context, returned to automatic mode afterwards."""
-    yield ctx
-    ctx.set_iteration_mode(N.ITER_AUTO)
-
-
-MODE_CASES = {
-    "cd2d_64": lambda: W.convdiff2d(64, 10.0),
-    "circuit": lambda: W.circuit_like(),
-    "cd3d_24": lambda: W.convdiff3d(24, 20.0),
-}
-
-
-@pytest.mark.parametrize("case", list(MODE_CASES))
-def test_graph_and_persistent_iterations(mode_ctx, case):
-    """The persistent kernel (one cooperative launch, grid barriers) and the
-    graph of fused kernels follow the same recurrences with dot products summed
-    in different orders: in FP64 the two are within +-1 of each other and of
-    the oracle; with FP32 Krylov vectors that rounding moves an irregular
-    problem by a few iterations (within 5%); the residual is below the
-    tolerance either way."""
-    A = MODE_CASES[case]()
-    b, _ = W.rhs_from_solution(A, seed=11)
-    m_o, _, _, _ = oracle.spai(A, "mgs")
-    ref = oracle.bicgstab(A, m_o, b, None, tol=1e-8, tol_mode="rel", maxiter=1000)
-    for prec in (N.PREC_FP64, N.PREC_M_BF16, N.PREC_MIXED_FP32):
-        its = {}
-        for mode in (N.ITER_GRAPH, N.ITER_PERSISTENT):
-            mode_ctx.set_iteration_mode(mode)
-            x, _, _, si = mode_ctx.solve_h(A, b, precision=prec)
-            assert si.status == N.SOLVE_CONVERGED, (mode, prec, si.status)
-            assert np.linalg.norm(b - A.matvec(x)) / np.linalg.norm(b) < 1e-8
-            its[mode] = si.iters
-        slack = 1 if prec in (N.PREC_FP64, N.PREC_M_BF16) else max(1, round(0.05 * its[N.ITER_GRAPH]))
-        assert abs(its[N.ITER_GRAPH] - its[N.ITER_PERSISTENT]) <= slack, (prec, its)
-        if prec == N.PREC_FP64:
-            assert abs(its[N.ITER_PERSISTENT] - ref["iters"]) <= 1
-
-
-def test_persistent_reference_settings_and_counter(mode_ctx):
-    """b = 1, x0 = 1, absolute 1e-7, no verification (runBiCGSTABOnRank0), and
-    the counter at maxiter, on the persistent path."""
-    mode_ctx.set_iteration_mode(N.ITER_PERSISTENT)
-    A = W.convdiff2d(64, 10.0)
-    m_o, _, _, _ = oracle.spai(A, "mgs")
-    ref = oracle.bicgstab(A, m_o, np.ones(A.n), np.ones(A.n), tol=1e-7, tol_mode="abs", maxiter=10000)
-    m, _, _ = mode_ctx.build_h(A)
-    x, info = mode_ctx.bicgstab_h(A, m, np.ones(A.n), np.ones(A.n), tol=1e-7, tol_mode=N.TOL_ABS, maxiter=10000,
-                                  verify=0)
-    assert info.status == N.SOLVE_CONVERGED and abs(info.iters - ref["iters"]) <= 1
-    b = W.rhs_ones_product(A)
-    x, info = mode_ctx.bicgstab_h(A, m, b, maxiter=5, tol=1e-30, verify=0)
-    assert info.status == N.SOLVE_MAXITER and info.iters == 5
-
-
-def test_iteration_mode_rejects_unknown(mode_ctx):
-    from dcu_b200.api import DcuError
-
-    with pytest.raises(DcuError):
-        mode_ctx.set_iteration_mode(7)
