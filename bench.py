@@ -417,6 +417,10 @@ def main():
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
     hp, hi, hv, hb = pin(A.ptr), pin(A.idx), pin(A.val), pin(b_h)
     hx = pin(np.zeros(n))
+    for _ in range(args.warmup):  # first calls size the upload buffer
+        hx[:] = 0.0
+        ctx.solve_h_into(n, nnz, hp, hi, hv, hb, hx, precision=head)
+    torch.cuda.synchronize(dev)
     e2e_ms = []
     for i in range(max(1, steps)):
         hx[:] = 0.0

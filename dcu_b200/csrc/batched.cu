@@ -431,9 +431,10 @@ __global__ void __launch_bounds__(BT) kb_az(BArgs<R> a) {
     for (int qq = 0; qq < R; ++qq) {
       const int i = sys * R + qq;
       if (!a.st.active[i]) continue;
-      const double omega = tot[0 * R + qq] / tot[1 * R + qq];
+      // Az = 0 (s = 0 when the half step solved the pair): omega = 0
+      const double omega = (tot[1 * R + qq] == 0.0) ? 0.0 : tot[0 * R + qq] / tot[1 * R + qq];
       a.st.omega[i] = omega;
-      if (tot[1 * R + qq] == 0.0 || omega == 0.0 || !isfinite(omega)) {
+      if (!isfinite(omega)) {
         a.st.active[i] = 0;
         a.st.status[i] = DCU_SOLVE_BREAKDOWN;
         a.st.alpha[i] = a.st.omega[i] = a.st.beta[i] = 0.0;
@@ -499,12 +500,16 @@ __global__ void __launch_bounds__(BT) kb_xr(BArgs<R> a) {
       a.st.beta[i] = beta;
       a.st.res[i] = sqrt(tot[1 * R + qq]);
       a.st.conv_it[i] = it;
-      if (!isfinite(a.st.res[i]) || !isfinite(beta) || rho_new == 0.0) {
+      // the stop test first, as in the reference (it never examines beta)
+      if (!isfinite(a.st.res[i])) {
         a.st.active[i] = 0;
         a.st.status[i] = DCU_SOLVE_BREAKDOWN;
       } else if (a.st.res[i] < a.st.thr[i]) {
         a.st.active[i] = 0;
         a.st.status[i] = DCU_SOLVE_CONVERGED;
+      } else if (!isfinite(beta) || rho_new == 0.0) {
+        a.st.active[i] = 0;
+        a.st.status[i] = DCU_SOLVE_BREAKDOWN;
       } else if (it + 1 >= a.g->maxiter) {
         a.st.status[i] = DCU_SOLVE_MAXITER;
         a.st.conv_it[i] = it + 1;

@@ -376,9 +376,11 @@ __global__ void __launch_bounds__(BI_BLOCK) k_bi_az(BiArgs<MT, IT, VT> a) {
   double tot[2];
   if (grid_reduce<2>(v, a.part, &a.S->counter[2], tot) && threadIdx.x == 0) {
     Scal* S = a.S;
-    const double omega = tot[0] / tot[1];
+    // Az = 0 (s = 0 when the half step solved the system): omega = 0, and K5
+    // finds r = s; the reference's 0 / 0 would make x NaN
+    const double omega = (tot[1] == 0.0) ? 0.0 : tot[0] / tot[1];
     S->omega = omega;
-    if (tot[1] == 0.0 || omega == 0.0 || bad(omega)) {
+    if (bad(omega)) {
       S->status = DCU_SOLVE_BREAKDOWN;
       S->done = 1;
     }
@@ -432,12 +434,16 @@ __global__ void __launch_bounds__(BI_BLOCK, 6) k_bi_xr(BiArgs<MT, IT, VT> a) {
     S->rho = rho_new;
     S->res = sqrt(tot[1]);
     S->pidx ^= 1;
-    if (bad(S->res) || bad(beta) || rho_new == 0.0) {
+    // the stop test first, as in the reference (it never examines beta)
+    if (bad(S->res)) {
       S->status = DCU_SOLVE_BREAKDOWN;
       S->done = 1;
     } else if (S->res < S->thr) {
       if (S->verify) S->verify_pending = 1;
       else S->status = DCU_SOLVE_CONVERGED;
+      S->done = 1;
+    } else if (bad(beta) || rho_new == 0.0) {
+      S->status = DCU_SOLVE_BREAKDOWN;
       S->done = 1;
     } else {
       S->it += 1;

@@ -90,7 +90,10 @@ typedef enum {
 typedef enum {
   DCU_SOLVE_CONVERGED = 0,
   DCU_SOLVE_MAXITER = 1,
-  DCU_SOLVE_BREAKDOWN = 2 /* rho, (r*,Ay), (Az,Az) or omega zero / non-finite */
+  DCU_SOLVE_BREAKDOWN = 2 /* rho or (r*,Ay) zero, a non-finite scalar or residual, or
+                             beta undefined (omega = 0) while ||r|| is above the threshold.
+                             (Az,Az) = 0 gives omega = 0: when the half step solved the
+                             system, r = s meets the threshold and the solve converges. */
 } dcu_solve_status;
 
 typedef struct {
