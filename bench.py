@@ -412,6 +412,47 @@ def main():
     it_gbs = sum(kbytes) / (it_us * 1e-6) / 1e9
     roofline["iteration"] = {"bytes": int(sum(kbytes)), "us": round(it_us, 1), "achieved": round(it_gbs, 1),
                              "frac": round(it_gbs / peak, 3)}
+    # the plain FP64 form's iteration on the same layout, and both forms' whole
+    # solve: SPAI build bytes (12 nnz + 4 (n + 1) read, 8 nnz of M written) plus
+    # iterations x iteration bytes, over the timed ms
+    pbytes = sum(bytes_per_kernel(n, nnz, 8, 8, index_bytes(n, 4, slots, uslots)))
+    pl_last = inf_plain[-1]
+    p_us = pl_last[1].ms * 1e3 / max(1, pl_last[1].iters)
+    p_gbs = pbytes / (p_us * 1e-6) / 1e9
+    roofline["plain_iteration"] = {"bytes": int(pbytes), "us": round(p_us, 1), "achieved": round(p_gbs, 1),
+                                   "frac": round(p_gbs / peak, 3)}
+    b_spai = 12 * nnz + 4 * (n + 1) + 8 * nnz
+    whole = {}
+    for name, it_b, info, tms in ((args.form, sum(kbytes), inf_head[-1], statistics.mean(ms_head)),
+                                  ("fp64", pbytes, pl_last, statistics.mean(ms_plain))):
+        tot_b = b_spai + info[1].iters * it_b
+        whole[name] = {"bytes": int(tot_b), "ms": round(tms, 3),
+                       "frac": round(tot_b / (tms * 1e-3) / 1e9 / peak, 3)}
+    roofline["whole_solve"] = whole
+
+    # Error of each result against an FP64 reference solve on the GPU (FP64
+    # SPAI + FP64 BiCGSTAB to 1e-12) and against the manufactured x_true, and
+    # the SPAI column residuals max_k ||A m_k - e_k|| of the headline and FP64
+    # builds (outside the timed region; after the per-kernel timer, which
+    # times the last solve on the context).
+    errors = None
+    if not args.profile_only:
+        x_ref = torch.zeros(n, dtype=torch.float64, device=dev)
+        ctx.solve_d(n, nnz, ptr, idx, val, b, x_ref, mval_d=mval, precision=FORMS["fp64"], tol=1e-12, maxiter=3000)
+        xr = x_ref.cpu().numpy()
+        nr, nt = float(np.linalg.norm(xr)), float(np.linalg.norm(xt))
+        colres = torch.zeros(n, dtype=torch.float64, device=dev)
+        cmax = {}
+        for name in (args.form, "fp64"):
+            ctx.build_d(n, nnz, ptr, idx, val, mval, colres, precision=FORMS[name])
+            cmax[name] = float(colres.max().item())
+        errors = {"ref": "FP64 SPAI + FP64 BiCGSTAB to 1e-12 relative (GPU)",
+                  "x_rel_err_vs_ref": {args.form: float(np.linalg.norm(xm - xr) / nr),
+                                       "fp64": float(np.linalg.norm(x_plain - xr) / nr)},
+                  "x_rel_err_vs_x_true": {args.form: float(np.linalg.norm(xm - xt) / nt),
+                                          "fp64": float(np.linalg.norm(x_plain - xt) / nt),
+                                          "ref": float(np.linalg.norm(xr - xt) / nt)},
+                  "max_column_residual": cmax}
 
     # end to end through the host-buffer entry point
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
@@ -478,6 +519,7 @@ def main():
                        "plain_fp64_ms": round(plain_v, 3), "plain_fp64_iters": pl_[1].iters,
                        "plain_fp64_build_ms": round(pl_[0].ms, 3), "plain_rel_res": relres_plain,
                        "speedup_vs_plain_fp64": round(plain_v / ms, 3),
+                       "errors": errors,
                        "forms": forms,
                        "ms_steps": [round(v, 3) for v in ms_head]},
             "e2e": {"value": round(e2e_v, 3), "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},

@@ -48,7 +48,9 @@ enum {
   ST_FB_COUNT = 10,   // columns the thread kernel hands to the group kernel
   ST_FB_HEAD = 11,    // queue head of that hand-off list
   ST_NE_COLS = 12,    // columns finished by the thread kernel
-  ST_INTS = 16,
+  ST_STAGE_FAIL = 13, // a bulk copy into shared memory did not complete in time
+  ST_STAGED = 16,     // CTA-kernel columns whose J columns were staged by bulk copies
+  ST_INTS = 24,
   ST_AREA64 = 7       // long long index (ints 14-15): max candidates * (|J|+1) over queued columns
 };
 
@@ -680,6 +682,9 @@ constexpr int LG_BLOCK = 256;
 constexpr int LG_WARPS = LG_BLOCK / 32;
 constexpr int LG_NJ_MAX = 2048;      // max |J_k| (J metadata lives in shared memory)
 constexpr int LG_WORDS_SMEM = 4096;  // bitmap words kept in shared memory
+constexpr int LG_STAGE_NJ = 256;     // J columns staged in shared memory by bulk copies
+constexpr int LG_STAGE_BYTES = 48 * 1024;
+constexpr long long kStageWaitSpins = 1ll << 22;
 
 struct LargeArgs {
   int n;
@@ -699,7 +704,44 @@ struct LargeArgs {
   void* gA;                // per block: area_per_block elements of T
   long long area_per_block;
   long long smem_area;     // elements of T that fit the shared slab
+  int stage_ok;            // idx (and val when building) 16-byte aligned: bulk copies allowed
 };
+
+// Bulk copies (the TMA engine, no multicast) of global ranges into this CTA's
+// shared memory, completing on an mbarrier.  Addresses and sizes are
+// multiples of 16 bytes.
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long* mbar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%1], %0;" : : "r"(count), "r"(smem_u32(mbar)) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_shared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* mbar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;" : : "r"(bytes), "r"(smem_u32(mbar))
+               : "memory");
+}
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* mbar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+               :
+               : "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(mbar))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* mbar, unsigned parity) {
+  unsigned done;
+  asm volatile(
+      "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, P1;\n\t}"
+      : "=r"(done)
+      : "r"(smem_u32(mbar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+// Bounded wait for the phase with the given parity; false when it gave up.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* mbar, unsigned parity) {
+  for (long long i = 0; i < kStageWaitSpins; ++i)
+    if (mbar_try_wait(mbar, parity)) return true;
+  return false;
+}
 
 template <typename T>
 struct LargeSmem {
@@ -712,6 +754,9 @@ struct LargeSmem {
   T rd[LG_NJ_MAX];
   double red[LG_WARPS];
   int ired[LG_WARPS * 2];
+  int jso[LG_STAGE_NJ + 1];  // staged int range of J column j starts at jso[j] ints
+  int jvo[LG_STAGE_NJ + 1];  // staged double range of J column j starts at jvo[j] doubles
+  unsigned long long mbar;   // completion of the bulk copies
   int col_q;
   int m;
   int E;
@@ -767,8 +812,16 @@ template <typename T, int MODE>
 __global__ void __launch_bounds__(LG_BLOCK, 1) k_spai_large(LargeArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   LargeSmem<T>& S = *reinterpret_cast<LargeSmem<T>*>(smem_raw);
-  T* sA = reinterpret_cast<T*>(smem_raw + ((sizeof(LargeSmem<T>) + 15) / 16) * 16);
+  // [LargeSmem][staging area][dense slab]
+  unsigned char* stage = smem_raw + ((sizeof(LargeSmem<T>) + 15) / 16) * 16;
+  T* sA = reinterpret_cast<T*>(stage + LG_STAGE_BYTES);
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  if (tid == 0) {
+    mbar_init(&S.mbar, 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  unsigned phase = 0;
   const int nbig = a.stats[ST_BIG_COUNT];
   unsigned* gbits = a.gbits + (long long)blockIdx.x * 2 * a.words_per_block;
   int* gpre = reinterpret_cast<int*>(gbits + a.words_per_block);
@@ -797,6 +850,58 @@ __global__ void __launch_bounds__(LG_BLOCK, 1) k_spai_large(LargeArgs a) {
     const int cand = block_scan(nj, [&](int i) { return S.jlen[i]; }, S.jcb, S.ired);
     if (tid == 0) S.jcb[nj] = cand;
     __syncthreads();
+    // Stage the J columns' row indices (and, when building, values) in shared
+    // memory with one bulk copy per column and array, each range rounded out
+    // to 16-byte boundaries, when they fit; the passes below then walk the
+    // columns in shared memory instead of locating every candidate in global
+    // memory.  The rounding never leaves the 16-byte block that holds an
+    // array's last element.
+    bool staged = false;
+    int* srow = reinterpret_cast<int*>(stage);
+    const double* sval = nullptr;
+    if (a.stage_ok && cand > 0 && nj <= LG_STAGE_NJ) {
+      const int rtot = block_scan(nj, [&](int i) {
+        const int b = S.jbase[i];
+        return ((b + S.jlen[i] + 3) & ~3) - (b & ~3);
+      }, S.jso, S.ired);
+      // values only when building (the pattern modes have no value array)
+      const int vtot = (MODE == MODE_BUILD) ? block_scan(nj, [&](int i) {
+        const int b = S.jbase[i];
+        return ((b + S.jlen[i] + 1) & ~1) - (b & ~1);
+      }, S.jvo, S.ired) : 0;
+      const long long bytes = 4ll * rtot + 8ll * vtot;
+      if (bytes > 0 && bytes <= LG_STAGE_BYTES) {
+        staged = true;
+        sval = reinterpret_cast<const double*>(stage + 4ll * rtot);
+        if (tid == 0) mbar_arrive_expect_tx(&S.mbar, (unsigned)bytes);
+        fence_async_shared();  // earlier reads of the staging area come first
+        __syncthreads();       // the expected bytes are set before any copy lands
+        for (int t = tid; t < nj; t += LG_BLOCK) {
+          const int b = S.jbase[t], e = b + S.jlen[t];
+          const int rb = b & ~3, re = (e + 3) & ~3;
+          if (re > rb) bulk_copy_g2s(srow + S.jso[t], a.idx + rb, 4u * (unsigned)(re - rb), &S.mbar);
+          if (MODE == MODE_BUILD) {
+            const int vb = b & ~1, ve = (e + 1) & ~1;
+            if (ve > vb) bulk_copy_g2s((void*)(sval + S.jvo[t]), a.val + vb, 8u * (unsigned)(ve - vb), &S.mbar);
+          }
+        }
+        const bool ok = mbar_wait(&S.mbar, phase);
+        phase ^= 1u;
+        if (__syncthreads_or(!ok)) {
+          // give the copies in flight a second bounded wait, report, stop
+          if (tid == 0) {
+            mbar_wait(&S.mbar, phase ^ 1u);
+            atomicAdd(&a.stats[ST_STAGE_FAIL], 1);
+          }
+          __syncthreads();
+          return;
+        }
+        if (MODE == MODE_BUILD && tid == 0) atomicAdd(&a.stats[ST_STAGED], 1);
+      }
+    }
+    // row / value of entry q of J column j in the staged copy
+    auto srow_at = [&](int j, int q) { return srow[S.jso[j] + (S.jbase[j] & 3) + q]; };
+    auto sval_at = [&](int j, int q) { return sval[S.jvo[j] + (S.jbase[j] & 1) + q]; };
     // candidate enumeration: candidate t -> (column slot j, position src)
     auto locate = [&](int t, int& j, int& src) {
       int lo = 0, hi = nj - 1;
@@ -809,12 +914,21 @@ __global__ void __launch_bounds__(LG_BLOCK, 1) k_spai_large(LargeArgs a) {
       src = S.jbase[lo] + (t - S.jcb[lo]);
     };
     int rmin = INT_MAX, rmax = -1;
-    for (int t = tid; t < cand; t += LG_BLOCK) {
-      int j, src;
-      locate(t, j, src);
-      const int row = a.idx[src];
-      rmin = min(rmin, row);
-      rmax = max(rmax, row);
+    if (staged) {
+      for (int j = wid; j < nj; j += LG_WARPS)
+        for (int q = lane; q < S.jlen[j]; q += 32) {
+          const int row = srow_at(j, q);
+          rmin = min(rmin, row);
+          rmax = max(rmax, row);
+        }
+    } else {
+      for (int t = tid; t < cand; t += LG_BLOCK) {
+        int j, src;
+        locate(t, j, src);
+        const int row = a.idx[src];
+        rmin = min(rmin, row);
+        rmax = max(rmax, row);
+      }
     }
 #pragma unroll
     for (int d = 16; d > 0; d >>= 1) {
@@ -840,11 +954,19 @@ __global__ void __launch_bounds__(LG_BLOCK, 1) k_spai_large(LargeArgs a) {
     int* wpre = (words <= LG_WORDS_SMEM) ? S.wpre : gpre;
     for (int w = tid; w < words; w += LG_BLOCK) bits[w] = 0u;
     __syncthreads();
-    for (int t = tid; t < cand; t += LG_BLOCK) {
-      int j, src;
-      locate(t, j, src);
-      const int off = a.idx[src] - rmin;
-      atomicOr(&bits[off >> 5], 1u << (off & 31));
+    if (staged) {
+      for (int j = wid; j < nj; j += LG_WARPS)
+        for (int q = lane; q < S.jlen[j]; q += 32) {
+          const int off = srow_at(j, q) - rmin;
+          atomicOr(&bits[off >> 5], 1u << (off & 31));
+        }
+    } else {
+      for (int t = tid; t < cand; t += LG_BLOCK) {
+        int j, src;
+        locate(t, j, src);
+        const int off = a.idx[src] - rmin;
+        atomicOr(&bits[off >> 5], 1u << (off & 31));
+      }
     }
     __syncthreads();
     const int m = block_scan(words, [&](int w) { return __popc(bits[w]); }, wpre, S.ired);
@@ -890,10 +1012,15 @@ __global__ void __launch_bounds__(LG_BLOCK, 1) k_spai_large(LargeArgs a) {
       S.E = E;
     }
     __syncthreads();
-    for (int t = tid; t < cand; t += LG_BLOCK) {
-      int j, src;
-      locate(t, j, src);
-      Ad[(long long)j * lda + rank(a.idx[src])] = (T)a.val[src];
+    if (staged) {
+      for (int j = wid; j < nj; j += LG_WARPS)
+        for (int q = lane; q < S.jlen[j]; q += 32) Ad[(long long)j * lda + rank(srow_at(j, q))] = (T)sval_at(j, q);
+    } else {
+      for (int t = tid; t < cand; t += LG_BLOCK) {
+        int j, src;
+        locate(t, j, src);
+        Ad[(long long)j * lda + rank(a.idx[src])] = (T)a.val[src];
+      }
     }
     if (tid == 0 && S.E >= 0) Ad[(long long)nj * lda + S.E] = T(1);
     __syncthreads();
@@ -1006,8 +1133,11 @@ int run_small(Ctx* c, SmallArgs a, int) {
 
 template <typename T, int MODE>
 int run_large(Ctx* c, LargeArgs& a, int nbig) {
-  const size_t fixed = ((sizeof(LargeSmem<T>) + 15) / 16) * 16;
+  const size_t fixed = ((sizeof(LargeSmem<T>) + 15) / 16) * 16 + LG_STAGE_BYTES;
   size_t cap = c->smem_optin > fixed + 1024 ? c->smem_optin - 1024 : fixed;
+  // bulk copies read idx (every mode) and val (build only) in 16-byte units
+  a.stage_ok = (a.idx && reinterpret_cast<uintptr_t>(a.idx) % 16 == 0 &&
+                (MODE != MODE_BUILD || (a.val && reinterpret_cast<uintptr_t>(a.val) % 16 == 0))) ? 1 : 0;
   a.smem_area = (MODE == MODE_BUILD) ? (long long)((cap - fixed) / sizeof(T)) : 0;
   const size_t smem = fixed + (size_t)a.smem_area * sizeof(T);
   DCU_CUDA(c, cudaFuncSetAttribute(k_spai_large<T, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1144,6 +1274,7 @@ int build_typed(Ctx* c, int n, const int* ptr, const int* idx, const double* val
     DCU_TRY((run_large<T, MODE_BUILD>(c, la, nbig)));
     DCU_TRY(read_stats(c, st));
     if (st[ST_LIMIT] > 0) return fail(c, DCU_ERR_LIMIT, "%d columns exceeded the CTA kernel's limits", st[ST_LIMIT]);
+    if (st[ST_STAGE_FAIL] > 0) return fail(c, DCU_ERR_CUDA, "a bulk copy into shared memory did not complete");
   }
   if (info) {
     info->cols_total = col_end - col_start;
@@ -1152,6 +1283,7 @@ int build_typed(Ctx* c, int n, const int* ptr, const int* idx, const double* val
     info->cols_singular = st[ST_SINGULAR];
     info->max_nj = st[ST_MAXNJ] > st[ST_BIG_MAXNJ] ? st[ST_MAXNJ] : st[ST_BIG_MAXNJ];
     info->max_ni = st[ST_MAXNI];
+    info->cols_staged = st[ST_STAGED];
   }
   return DCU_OK;
 }
@@ -1219,6 +1351,8 @@ int spai_pattern(Ctx* c, int n, const int* ptr, const int* idx, int col_start, i
       la.stats = P.stats;
       if (pass == 0) DCU_TRY((run_large<double, MODE_COUNT>(c, la, st[ST_BIG_COUNT])));
       else DCU_TRY((run_large<double, MODE_LIST>(c, la, st[ST_BIG_COUNT])));
+      DCU_TRY(read_stats(c, st));
+      if (st[ST_STAGE_FAIL] > 0) return fail(c, DCU_ERR_CUDA, "a bulk copy into shared memory did not complete");
     }
     if (pass == 0) {
       DCU_TRY(scan_exclusive_i64(c, icount, iptr, ncols));

@@ -34,7 +34,8 @@ class Options(C.Structure):
 
 class BuildInfo(C.Structure):
     _fields_ = [("cols_total", C.c_int), ("cols_small", C.c_int), ("cols_large", C.c_int),
-                ("cols_singular", C.c_int), ("max_nj", C.c_int), ("max_ni", C.c_int), ("ms", C.c_float)]
+                ("cols_singular", C.c_int), ("max_nj", C.c_int), ("max_ni", C.c_int), ("ms", C.c_float),
+                ("cols_staged", C.c_int)]
 
 
 class SolveInfo(C.Structure):

@@ -104,6 +104,8 @@ typedef struct {
   int max_nj;             /* max |J_k|                                            */
   int max_ni;             /* max |I_k|                                            */
   float ms;               /* device time of the build (CUDA events)              */
+  int cols_staged;        /* CTA-kernel columns whose J columns were brought into
+                             shared memory by bulk (TMA) copies                    */
 } dcu_build_info;
 
 typedef struct {

@@ -112,3 +112,34 @@ def test_spai_fp64_normal_equations(ctx, name, A):
     m, res, info = ctx.build_h(A, precision=N.PREC_FP64, ls_method=N.LS_NORMAL_EQ)
     assert info.cols_small + info.cols_large == A.n
     assert rel_err(m, m_h) < 1e-9
+
+
+def test_bulk_copy_staging_matches_plain_loads(ctx):
+    """The CTA kernel stages its J columns in shared memory with bulk (TMA)
+    copies when A's arrays are 16-byte aligned, and reads them from global
+    memory otherwise; both give the same M, bit for bit, equal to the oracle's
+    within 1e-10.  The pattern kernel (no value array) stages indices only."""
+    import torch
+
+    A = W.circuit_like()
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    ptr = d(A.ptr)
+    idx, val = d(A.idx), d(A.val)
+    # the same arrays 4 / 8 bytes past a 16-byte boundary: no bulk copies
+    idx_u = torch.empty(A.nnz + 1, dtype=torch.int32, device="cuda")[1:]
+    val_u = torch.empty(A.nnz + 1, dtype=torch.float64, device="cuda")[1:]
+    idx_u.copy_(idx)
+    val_u.copy_(val)
+    assert idx_u.data_ptr() % 16 != 0 and val_u.data_ptr() % 16 != 0
+    m1 = torch.zeros(A.nnz, dtype=torch.float64, device="cuda")
+    m2 = torch.zeros_like(m1)
+    i1 = ctx.build_d(A.n, A.nnz, ptr, idx, val, m1)
+    i2 = ctx.build_d(A.n, A.nnz, ptr, idx_u, val_u, m2)
+    assert i1.cols_large > 0 and i1.cols_staged > 0 and i2.cols_staged == 0
+    assert torch.equal(m1, m2)
+    m_o, _, _, _ = oracle.spai(A, "mgs")
+    mh = m1.cpu().numpy()
+    assert np.max(np.abs(mh - m_o)) <= 1e-10 * np.max(np.abs(m_o))
+    c1, p1, l1 = ctx.pattern_d(A.n, ptr, idx)
+    c2, p2, l2 = ctx.pattern_d(A.n, ptr, idx_u)
+    assert torch.equal(c1, c2) and torch.equal(l1, l2)
