@@ -50,10 +50,12 @@ def workload(m=128, pe=20.0):
     return A, b, xt
 
 
-def iteration_kernels(w_m):
+def iteration_kernels(split):
     """Names of the iteration kernels in launch order: K1 is split in two
-    (streaming p update + one-vector SpMV) when M is narrower than FP64."""
-    k1 = ["k_bi_p", "k_bi_y"] if w_m < 8 else ["k_bi_py"]
+    (streaming p update + one-vector SpMV) or fused (p formed at every
+    gathered column); narrow M forms split by default, the autotuner may
+    choose either where both compute the same values."""
+    k1 = ["k_bi_p", "k_bi_y"] if split else ["k_bi_py"]
     return k1 + ["k_bi_ay", "k_bi_sz", "k_bi_az", "k_bi_xr"]
 
 
@@ -64,10 +66,10 @@ def index_bytes(n, w_i, slots, uniform_slots):
     return w_i * (slots - uniform_slots) + 4 * (uniform_slots // 32) + 12 * ((n + 31) // 32)
 
 
-def bytes_per_kernel(n, nnz, w_m, w_v, ib):
+def bytes_per_kernel(n, nnz, w_m, w_v, ib, split):
     """Algorithmic HBM bytes of each iteration kernel (one launch), in the
-    order of iteration_kernels(); ib = index_bytes() of one SpMV."""
-    if w_m < 8:
+    order of iteration_kernels(split); ib = index_bytes() of one SpMV."""
+    if split:
         k1 = [n * (16 + 2 * w_v),                           # K1a p = r + beta(p - w ay)
               nnz * w_m + ib + n * 2 * w_v]                 # K1b y = M p
     else:
@@ -293,6 +295,7 @@ def main():
     ap.add_argument("--workload", default="cd3d128", choices=["cd3d128", "batch512", "grad512"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-only", action="store_true", help="one plain + one headline solve, no timing loop")
+    ap.add_argument("--no-autotune", action="store_true", help="default launch configuration (no dcu_autotune_d)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -355,6 +358,13 @@ def main():
         ms = [a.elapsed_time(z) for a, z in ev]
         return ms, infos, ctx.launches - l0
 
+    # the autotuner picks each reported form's launch configuration once,
+    # before the warm-up (its choice never changes a form's solution bits)
+    tuning = {}
+    if not args.no_autotune:
+        for name in dict.fromkeys((args.form, "fp64")):
+            tu = ctx.autotune_d(n, nnz, ptr, idx, val, b, reps=10, precision=FORMS[name]).as_dict()
+            tuning[name] = {k: (round(v, 3) if isinstance(v, float) else v) for k, v in tu.items()}
     for _ in range(args.warmup):
         solve(head)
         solve(FORMS["fp64"])
@@ -387,9 +397,10 @@ def main():
 
     # per-kernel timing of the headline form's iteration kernels (after its solve)
     kms = ctx.profile_iteration(reps=20)
+    split = len(kms) == 6
     w_m, w_v, w_i = form_widths(head)
     slots, uslots = ctx.sell_plan_stats()
-    kbytes = bytes_per_kernel(n, nnz, w_m, w_v, index_bytes(n, w_i, slots, uslots))
+    kbytes = bytes_per_kernel(n, nnz, w_m, w_v, index_bytes(n, w_i, slots, uslots), split)
     j = int(np.argmax(kms))
     peaks = {}
     try:
@@ -398,7 +409,7 @@ def main():
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = kbytes[j] / (kms[j] * 1e-3) / 1e9
-    names = iteration_kernels(w_m)
+    names = iteration_kernels(split)
     assert len(names) == len(kms) == len(kbytes), (names, kms)
     roofline = {"bound": "hbm", "kernel": names[j],
                 "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 3),
@@ -415,7 +426,9 @@ def main():
     # the plain FP64 form's iteration on the same layout, and both forms' whole
     # solve: SPAI build bytes (12 nnz + 4 (n + 1) read, 8 nnz of M written) plus
     # iterations x iteration bytes, over the timed ms
-    pbytes = sum(bytes_per_kernel(n, nnz, 8, 8, index_bytes(n, 4, slots, uslots)))
+    # (with the fused first step's bytes, the fewer of the two, whichever
+    # step the autotuner picked)
+    pbytes = sum(bytes_per_kernel(n, nnz, 8, 8, index_bytes(n, 4, slots, uslots), False))
     pl_last = inf_plain[-1]
     p_us = pl_last[1].ms * 1e3 / max(1, pl_last[1].iters)
     p_gbs = pbytes / (p_us * 1e-6) / 1e9
@@ -521,6 +534,7 @@ def main():
                        "speedup_vs_plain_fp64": round(plain_v / ms, 3),
                        "errors": errors,
                        "forms": forms,
+                       "tuning": tuning or None,
                        "ms_steps": [round(v, 3) for v in ms_head]},
             "e2e": {"value": round(e2e_v, 3), "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,

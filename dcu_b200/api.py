@@ -162,6 +162,36 @@ class Context:
         self._check(self._L.dcu_sell_plan_stats(self.h, C.byref(s), C.byref(u)))
         return s.value, u.value
 
+    def autotune_d(self, n, nnz, ptr_d, idx_d, val_d, b_d, reps: int = 10, **opt) -> "N.Tuning":
+        """Time the launch configurations of opt's precision form on this matrix and keep the fastest
+        for later builds and solves of that form on this context (dcu_autotune_d)."""
+        o = N.default_options(**opt)
+        t = N.Tuning()
+        self._check(self._L.dcu_autotune_d(self.h, n, nnz, _p(ptr_d), _p(idx_d), _p(val_d), _p(b_d), C.byref(o),
+                                           reps, C.byref(t)))
+        return t
+
+    def set_tuning(self, precision: int, tuning: "N.Tuning | None" = None, **fields):
+        """Pin a launch configuration for one precision form (None and no fields: back to the defaults)."""
+        if tuning is None and not fields:
+            self._check(self._L.dcu_set_tuning(self.h, precision, None))
+            return
+        t = N.Tuning()
+        if tuning is not None:
+            C.pointer(t)[0] = tuning
+        else:
+            self._L.dcu_tuning_default(C.byref(t))
+        for k, v in fields.items():
+            if k not in N.Tuning.CONFIG:
+                raise KeyError(k)
+            setattr(t, k, v)
+        self._check(self._L.dcu_set_tuning(self.h, precision, C.byref(t)))
+
+    def get_tuning(self, precision: int) -> "N.Tuning":
+        t = N.Tuning()
+        self._check(self._L.dcu_get_tuning(self.h, precision, C.byref(t)))
+        return t
+
     def csc_to_csr_d(self, n, nnz, ptr_d, idx_d, val_d, rptr_d, ridx_d, rval_d):
         self._check(self._L.dcu_csc_to_csr_d(self.h, n, nnz, _p(ptr_d), _p(idx_d), _p(val_d), _p(rptr_d),
                                              _p(ridx_d), _p(rval_d)))

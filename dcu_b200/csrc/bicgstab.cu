@@ -23,6 +23,7 @@
 //          the rho/alpha/omega/beta recurrences stay FP64.  x and r are updated
 //          with exactly the y, z, A y, A z that were stored, so the recurrence
 //          residual tracks b - A x to FP64 rounding.
+#include <array>
 #include <cmath>
 #include <algorithm>
 #include <cstddef>
@@ -509,30 +510,65 @@ cudaError_t launch_pdl(K kernel, int grid, cudaStream_t st, const A& args) {
   return cudaLaunchKernelEx(&cfg, kernel, args);
 }
 
+// Grid of a grid-stride kernel over `items` rows (or row pairs) for a tuning
+// selector: 0 one wave of `per_sm` resident blocks per SM, -1 one block per
+// BI_BLOCK items (no loop), k > 0 k blocks per SM (at most `per_sm`).
+int grid_for(const Ctx* c, long long items, int per_sm, int sel) {
+  if (sel < 0) return (int)std::max(1LL, (items + BI_BLOCK - 1) / BI_BLOCK);
+  return waves_grid(c, items, BI_BLOCK, sel > 0 ? std::min(sel, per_sm) : per_sm);
+}
+
 template <typename MT, typename IT, typename VT>
 int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval, const IT* ix, const double* b,
-               double* x, const dcu_options* opt, dcu_solve_info* info) {
+               double* x, const dcu_options* opt, const dcu_tuning* tu, dcu_solve_info* info) {
   const int n = plan.n;
-  // one full wave per kernel: as many blocks as are resident at once
-  auto gsize = [&](const void* fn) {
+  // blocks of each kernel resident on one SM at once
+  auto resident = [&](const void* fn) {
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, BI_BLOCK, 0) != cudaSuccess || per_sm < 1) {
       cudaGetLastError();
       per_sm = 1;
     }
-    return waves_grid(c, n, BI_BLOCK, per_sm);
+    return per_sm;
   };
-  const int g_init = gsize((const void*)k_bi_init<MT, IT, VT>);
-  const int g_py = gsize((const void*)k_bi_py<MT, IT, VT>);
-  const int g_ay = gsize((const void*)k_bi_ay<MT, IT, VT>);
-  const int g_sz = gsize((const void*)k_bi_sz<MT, IT, VT>);
-  const int g_az = gsize((const void*)k_bi_az<MT, IT, VT>);
-  const int g_xr = gsize((const void*)k_bi_xr<MT, IT, VT>);
-  const int g_tr = gsize((const void*)k_bi_true<MT, IT, VT>);
-  const int g_p = gsize((const void*)k_bi_p<MT, IT, VT>);
-  const int g_y = gsize((const void*)k_bi_y<MT, IT, VT>);
-  const int grid = std::max({g_init, g_py, g_ay, g_sz, g_az, g_xr, g_tr, g_p, g_y});  // partial-sum slots
-  constexpr bool split = split_k1<MT>();
+  std::array<int, IK_COUNT> rs;
+  rs[IK_P] = resident((const void*)k_bi_p<MT, IT, VT>);
+  rs[IK_Y] = resident((const void*)k_bi_y<MT, IT, VT>);
+  rs[IK_PY] = resident((const void*)k_bi_py<MT, IT, VT>);
+  rs[IK_AY] = resident((const void*)k_bi_ay<MT, IT, VT>);
+  rs[IK_SZ] = resident((const void*)k_bi_sz<MT, IT, VT>);
+  rs[IK_AZ] = resident((const void*)k_bi_az<MT, IT, VT>);
+  rs[IK_XR] = resident((const void*)k_bi_xr<MT, IT, VT>);
+  // rows each kernel's threads stride over (the p pass takes row pairs); the
+  // kernels that end in a reduction keep one full wave over n, whatever the
+  // tuning: their grid fixes the summation order of the partial sums
+  std::array<long long, IK_COUNT> items = {std::max(1, n >> 1), n, n, n, n, n, n};
+  std::array<int, IK_COUNT> sel = {0, 0, 0, 0, 0, 0, 0};
+  if (tu) {
+    sel[IK_P] = tu->grid_p;
+    sel[IK_Y] = tu->grid_y;
+    sel[IK_PY] = tu->grid_py;
+    sel[IK_SZ] = tu->grid_sz;
+  }
+  auto grid_of = [c, rs, items](int kind, int s) {
+    const bool tunable = kind == IK_P || kind == IK_Y || kind == IK_PY || kind == IK_SZ;
+    return grid_for(c, items[kind], rs[kind], tunable ? s : 0);
+  };
+  const int g_init = waves_grid(c, n, BI_BLOCK, resident((const void*)k_bi_init<MT, IT, VT>));
+  const int g_tr = waves_grid(c, n, BI_BLOCK, resident((const void*)k_bi_true<MT, IT, VT>));
+  const int g_p = grid_of(IK_P, sel[IK_P]);
+  const int g_y = grid_of(IK_Y, sel[IK_Y]);
+  const int g_py = grid_of(IK_PY, sel[IK_PY]);
+  const int g_ay = grid_of(IK_AY, 0);
+  const int g_sz = grid_of(IK_SZ, sel[IK_SZ]);
+  const int g_az = grid_of(IK_AZ, 0);
+  const int g_xr = grid_of(IK_XR, 0);
+  const int grid = std::max({g_init, g_ay, g_az, g_xr, g_tr});  // partial-sum slots
+  // The fused and the split first step compute bit-identical p and y when the
+  // vectors are FP64 (the fused step's p is exact in VT); with FP32 vectors
+  // the fused step multiplies by the unrounded p, so the form keeps its split.
+  constexpr bool k1_free = std::is_same<VT, double>::value;
+  const bool split = (k1_free && tu && tu->k1_split >= 0) ? tu->k1_split == 1 : split_k1<MT>();
   // vectors: r, ay, s, az (double) + rs, p0, p1, y, z (VT), 256-byte aligned
   auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
   const size_t nd = al(sizeof(double) * (size_t)n), nv = al(sizeof(VT) * (size_t)n);
@@ -574,6 +610,7 @@ int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval,
   // the key names the kernel instantiation too: the same buffers are reused
   // by every precision form
   std::vector<const void*> key = {(const void*)&k_bi_py<MT, IT, VT>, (const void*)(intptr_t)grid,
+                                  (const void*)(intptr_t)split,
                                   (const void*)(intptr_t)g_py, (const void*)(intptr_t)g_ay, (const void*)(intptr_t)g_sz,
                                   (const void*)(intptr_t)g_az, (const void*)(intptr_t)g_xr, (const void*)(intptr_t)g_p,
                                   (const void*)(intptr_t)g_y};
@@ -620,25 +657,31 @@ int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval,
   // Chunks are launched one ahead of the flag that is read back, so the GPU
   // never idles on the host; after convergence at most one chunk of
   // early-exit kernels runs.
-  c->profile_kernels = split ? 6 : 5;
-  c->profile_launch = [c, a, g_py, g_ay, g_sz, g_az, g_xr, g_p, g_y](int j) -> int {
+  if (split) {
+    c->profile_order = {IK_P, IK_Y, IK_AY, IK_SZ, IK_AZ, IK_XR};
+    c->profile_sel = {sel[IK_P], sel[IK_Y], 0, sel[IK_SZ], 0, 0};
+  } else {
+    c->profile_order = {IK_PY, IK_AY, IK_SZ, IK_AZ, IK_XR};
+    c->profile_sel = {sel[IK_PY], 0, sel[IK_SZ], 0, 0};
+  }
+  c->profile_k1_free = k1_free;
+  c->profile_default_split = split_k1<MT>() ? 1 : 0;
+  c->profile_launch = [c, a, grid_of](int kind, int s) -> int {
+    const int g = grid_of(kind, s);
     DCU_CUDA(c, cudaMemsetAsync(&a.S->done, 0, sizeof(int), c->stream));
-    if (split && j == 0) {
-      k_bi_p<MT, IT, VT><<<g_p, BI_BLOCK, 0, c->stream>>>(a);
-    } else if (split && j == 1) {
-      k_bi_y<MT, IT, VT><<<g_y, BI_BLOCK, 0, c->stream>>>(a);
-    } else {
-      switch (split ? j - 1 : j) {
-        case 0: k_bi_py<MT, IT, VT><<<g_py, BI_BLOCK, 0, c->stream>>>(a); break;
-        case 1: k_bi_ay<MT, IT, VT><<<g_ay, BI_BLOCK, 0, c->stream>>>(a); break;
-        case 2: k_bi_sz<MT, IT, VT><<<g_sz, BI_BLOCK, 0, c->stream>>>(a); break;
-        case 3: k_bi_az<MT, IT, VT><<<g_az, BI_BLOCK, 0, c->stream>>>(a); break;
-        default: k_bi_xr<MT, IT, VT><<<g_xr, BI_BLOCK, 0, c->stream>>>(a); break;
-      }
+    switch (kind) {
+      case IK_P: k_bi_p<MT, IT, VT><<<g, BI_BLOCK, 0, c->stream>>>(a); break;
+      case IK_Y: k_bi_y<MT, IT, VT><<<g, BI_BLOCK, 0, c->stream>>>(a); break;
+      case IK_PY: k_bi_py<MT, IT, VT><<<g, BI_BLOCK, 0, c->stream>>>(a); break;
+      case IK_AY: k_bi_ay<MT, IT, VT><<<g, BI_BLOCK, 0, c->stream>>>(a); break;
+      case IK_SZ: k_bi_sz<MT, IT, VT><<<g, BI_BLOCK, 0, c->stream>>>(a); break;
+      case IK_AZ: k_bi_az<MT, IT, VT><<<g, BI_BLOCK, 0, c->stream>>>(a); break;
+      default: k_bi_xr<MT, IT, VT><<<g, BI_BLOCK, 0, c->stream>>>(a); break;
     }
     DCU_LAUNCHED(c, "profile kernel");
     return DCU_OK;
   };
+  c->profile_grid = grid_of;
 
   Scal hs;
   Scal* pin = reinterpret_cast<Scal*>(c->pinned);
@@ -700,59 +743,138 @@ int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval,
 int bicgstab_solve(Ctx* c, const SellPlan& plan, const double* aval_sell, const void* mval_sell, const double* b,
                    double* x, const dcu_options* opt, dcu_solve_info* info) {
   const int p = opt->precision;
+  const dcu_tuning* tu = (p >= 0 && p < 5 && c->tune_set[p]) ? &c->tune[p] : nullptr;
   if (p == DCU_PREC_FP64)
-    return run_solver<double, int, double>(c, plan, aval_sell, (const double*)mval_sell, plan.idx, b, x, opt, info);
+    return run_solver<double, int, double>(c, plan, aval_sell, (const double*)mval_sell, plan.idx, b, x, opt, tu, info);
   const bool m32 = (p == DCU_PREC_MIXED_FP32 || p == DCU_PREC_M_FP32);
   const bool v32 = (p == DCU_PREC_MIXED_FP32 || p == DCU_PREC_MIXED_BF16);
   const float* mf = (const float*)mval_sell;
   const __nv_bfloat16* mb = (const __nv_bfloat16*)mval_sell;
   if (plan.delta16) {
-    if (m32) return v32 ? run_solver<float, int16_t, float>(c, plan, aval_sell, mf, plan.del, b, x, opt, info)
-                        : run_solver<float, int16_t, double>(c, plan, aval_sell, mf, plan.del, b, x, opt, info);
-    return v32 ? run_solver<__nv_bfloat16, int16_t, float>(c, plan, aval_sell, mb, plan.del, b, x, opt, info)
-               : run_solver<__nv_bfloat16, int16_t, double>(c, plan, aval_sell, mb, plan.del, b, x, opt, info);
+    if (m32) return v32 ? run_solver<float, int16_t, float>(c, plan, aval_sell, mf, plan.del, b, x, opt, tu, info)
+                        : run_solver<float, int16_t, double>(c, plan, aval_sell, mf, plan.del, b, x, opt, tu, info);
+    return v32 ? run_solver<__nv_bfloat16, int16_t, float>(c, plan, aval_sell, mb, plan.del, b, x, opt, tu, info)
+               : run_solver<__nv_bfloat16, int16_t, double>(c, plan, aval_sell, mb, plan.del, b, x, opt, tu, info);
   }
-  if (m32) return v32 ? run_solver<float, int, float>(c, plan, aval_sell, mf, plan.idx, b, x, opt, info)
-                      : run_solver<float, int, double>(c, plan, aval_sell, mf, plan.idx, b, x, opt, info);
-  return v32 ? run_solver<__nv_bfloat16, int, float>(c, plan, aval_sell, mb, plan.idx, b, x, opt, info)
-             : run_solver<__nv_bfloat16, int, double>(c, plan, aval_sell, mb, plan.idx, b, x, opt, info);
+  if (m32) return v32 ? run_solver<float, int, float>(c, plan, aval_sell, mf, plan.idx, b, x, opt, tu, info)
+                      : run_solver<float, int, double>(c, plan, aval_sell, mf, plan.idx, b, x, opt, tu, info);
+  return v32 ? run_solver<__nv_bfloat16, int, float>(c, plan, aval_sell, mb, plan.idx, b, x, opt, tu, info)
+             : run_solver<__nv_bfloat16, int, double>(c, plan, aval_sell, mb, plan.idx, b, x, opt, tu, info);
 }
 
-int profile_iteration(Ctx* c, int reps, float* ms, int cap, int* count) {
-  if (!c->profile_launch) return fail(c, DCU_ERR_ARG, "no solve has run on this context");
-  if (count) *count = c->profile_kernels;
-  if (cap < c->profile_kernels) return fail(c, DCU_ERR_ARG, "ms_out holds fewer entries than kernels");
-  if (reps < 1) reps = 1;
-  // cost of the stop-flag reset that precedes every launch
+namespace {
+
+// Mean device time (ms) of the stop-flag reset that precedes every profiled launch.
+int reset_ms(Ctx* c, int reps, float* out) {
   int* done = reinterpret_cast<int*>(c->buf[B_SCAL].p) + offsetof(Scal, done) / sizeof(int);
   DCU_CUDA(c, cudaEventRecord(c->ev[0], c->stream));
   for (int r = 0; r < reps; ++r) DCU_CUDA(c, cudaMemsetAsync(done, 0, sizeof(int), c->stream));
   DCU_CUDA(c, cudaEventRecord(c->ev[1], c->stream));
   DCU_CUDA(c, cudaEventSynchronize(c->ev[1]));
-  float reset = 0.f;
-  cudaEventElapsedTime(&reset, c->ev[0], c->ev[1]);
-  reset /= reps;
-  // Each timed launch follows an untimed launch of the kernel that precedes
-  // it in the iteration, so L2 holds what it holds in a solve (A alone is
-  // larger than L2; back-to-back launches of one kernel would find part of
-  // their own data there).
-  const int nk = c->profile_kernels;
-  for (int j = 0; j < nk; ++j) {
-    const int pred = (j + nk - 1) % nk;
-    DCU_TRY(c->profile_launch(j));  // warm-up
-    float total = 0.f;
-    for (int r = 0; r < reps; ++r) {
-      DCU_TRY(c->profile_launch(pred));
-      DCU_CUDA(c, cudaEventRecord(c->ev[0], c->stream));
-      DCU_TRY(c->profile_launch(j));
-      DCU_CUDA(c, cudaEventRecord(c->ev[1], c->stream));
-      DCU_CUDA(c, cudaEventSynchronize(c->ev[1]));
-      float t = 0.f;
-      cudaEventElapsedTime(&t, c->ev[0], c->ev[1]);
-      total += t;
-    }
-    ms[j] = total / reps - reset;
+  float t = 0.f;
+  cudaEventElapsedTime(&t, c->ev[0], c->ev[1]);
+  *out = t / reps;
+  return DCU_OK;
+}
+
+// Mean device time (ms) of `kind` at selector `sel`.  Each timed launch
+// follows an untimed launch of the kernel that precedes it in the iteration
+// (`pred` at `pred_sel`), so L2 holds what it holds in a solve (A alone is
+// larger than L2; back-to-back launches of one kernel would find part of
+// their own data there).
+int time_kernel(Ctx* c, int kind, int sel, int pred, int pred_sel, int reps, float reset, float* out) {
+  DCU_TRY(c->profile_launch(kind, sel));  // warm-up
+  float total = 0.f;
+  for (int r = 0; r < reps; ++r) {
+    DCU_TRY(c->profile_launch(pred, pred_sel));
+    DCU_CUDA(c, cudaEventRecord(c->ev[0], c->stream));
+    DCU_TRY(c->profile_launch(kind, sel));
+    DCU_CUDA(c, cudaEventRecord(c->ev[1], c->stream));
+    DCU_CUDA(c, cudaEventSynchronize(c->ev[1]));
+    float t = 0.f;
+    cudaEventElapsedTime(&t, c->ev[0], c->ev[1]);
+    total += t;
   }
+  *out = total / reps - reset;
+  return DCU_OK;
+}
+
+}  // namespace
+
+int profile_iteration(Ctx* c, int reps, float* ms, int cap, int* count) {
+  if (!c->profile_launch) return fail(c, DCU_ERR_ARG, "no solve has run on this context");
+  const int nk = (int)c->profile_order.size();
+  if (count) *count = nk;
+  if (cap < nk) return fail(c, DCU_ERR_ARG, "ms_out holds fewer entries than kernels");
+  if (reps < 1) reps = 1;
+  float reset = 0.f;
+  DCU_TRY(reset_ms(c, reps, &reset));
+  for (int j = 0; j < nk; ++j) {
+    const int pj = (j + nk - 1) % nk;
+    DCU_TRY(time_kernel(c, c->profile_order[j], c->profile_sel[j], c->profile_order[pj], c->profile_sel[pj], reps,
+                        reset, &ms[j]));
+  }
+  return DCU_OK;
+}
+
+int tune_iteration(Ctx* c, int reps, dcu_tuning* t, int* timed) {
+  if (!c->profile_launch) return fail(c, DCU_ERR_ARG, "no solve has run on this context");
+  if (reps < 1) reps = 10;
+  float reset = 0.f;
+  DCU_TRY(reset_ms(c, reps, &reset));
+  // the kernels without a reduction, each after its predecessor in the iteration
+  std::vector<std::pair<int, int>> kinds = {{IK_P, IK_XR}, {IK_Y, IK_P}, {IK_SZ, IK_AY}};
+  if (c->profile_k1_free) kinds.push_back({IK_PY, IK_XR});
+  float def[IK_COUNT] = {}, best[IK_COUNT] = {};
+  int best_sel[IK_COUNT] = {};
+  int n_timed = 0;
+  for (auto [kind, pred] : kinds) {
+    // candidates: one wave (the default), one block per 256 rows, half the
+    // resident blocks per SM; a candidate with the same grid as an earlier one
+    // is not timed again
+    std::vector<int> cands = {0, -1};
+    const int full = c->profile_grid(kind, 0);
+    for (int k = 1; k <= 32; ++k) {
+      if (c->profile_grid(kind, k) == full) {  // k reaches the resident count
+        if (k / 2 >= 1) cands.push_back(k / 2);
+        break;
+      }
+    }
+    std::vector<int> grids;
+    for (int s : cands) {
+      const int g = c->profile_grid(kind, s);
+      bool seen = false;
+      for (int h : grids) seen = seen || h == g;
+      if (seen) continue;
+      grids.push_back(g);
+      float ms = 0.f;
+      DCU_TRY(time_kernel(c, kind, s, pred, 0, reps, reset, &ms));
+      ++n_timed;
+      if (s == 0) {
+        def[kind] = best[kind] = ms;
+        best_sel[kind] = 0;
+      } else if (ms < 0.99f * best[kind]) {  // a change must win by more than 1%
+        best[kind] = ms;
+        best_sel[kind] = s;
+      }
+    }
+  }
+  const bool dsplit = c->profile_default_split != 0;
+  bool split = dsplit;
+  if (c->profile_k1_free) {
+    const float fused = best[IK_PY], sp = best[IK_P] + best[IK_Y];
+    if (dsplit ? fused < 0.99f * sp : sp < 0.99f * fused) split = !dsplit;
+    t->k1_split = split ? 1 : 0;
+  } else {
+    t->k1_split = -1;
+  }
+  t->grid_p = best_sel[IK_P];
+  t->grid_y = best_sel[IK_Y];
+  t->grid_py = c->profile_k1_free ? best_sel[IK_PY] : 0;
+  t->grid_sz = best_sel[IK_SZ];
+  t->iter_us_default = 1000.f * ((dsplit ? def[IK_P] + def[IK_Y] : def[IK_PY]) + def[IK_SZ]);
+  t->iter_us_tuned = 1000.f * ((split ? best[IK_P] + best[IK_Y] : best[IK_PY]) + best[IK_SZ]);
+  if (timed) *timed = n_timed;
   return DCU_OK;
 }
 

@@ -146,9 +146,222 @@ int upload(Ctx* c, int n, int nnz, const int* ptr, const int* idx, const double*
   return DCU_OK;
 }
 
+// Device time (ms) of one SPAI build under the context's current tuning.
+int timed_build(Ctx* c, int n, int nnz, const int* ptr, const int* idx, const double* val, const dcu_options& o,
+                double* m, dcu_build_info* bi, float* ms) {
+  DCU_CUDA(c, cudaEventRecord(c->ev[0], c->stream));
+  DCU_TRY(dcu::spai_build(c, n, nnz, ptr, idx, val, &o, m, nullptr, bi));
+  DCU_CUDA(c, cudaEventRecord(c->ev[1], c->stream));
+  DCU_CUDA(c, cudaEventSynchronize(c->ev[1]));
+  cudaEventElapsedTime(ms, c->ev[0], c->ev[1]);
+  return DCU_OK;
+}
+
+// Scratch of the autotuner, released by the caller.
+struct TuneScratch {
+  double* x = nullptr;
+  int* icount = nullptr;
+  long long* iptr = nullptr;
+};
+
+// The autotuner's steps (dcu_autotune_d): warp-group |I| limit, then the
+// iteration's launch configuration on the buffers of one solve.  The
+// context's tuning of o.precision is what each timed run uses.
+int autotune(Ctx* c, int n, int nnz, const int* ptr, const int* idx, const double* val, const double* b,
+             const dcu_options& o, int reps, dcu_tuning* t, TuneScratch* tmp) {
+  const int p = o.precision;
+  dcu_tuning_default(t);
+  c->tune[p] = *t;
+  c->tune_set[p] = true;
+  DCU_TRY(dcu::validate_csc(c, n, nnz, ptr, idx));
+  DCU_TRY(dcu::ensure(c, dcu::B_MVAL, sizeof(double) * (size_t)(nnz > 0 ? nnz : 1)));
+  double* m = dcu::bp<double>(c, dcu::B_MVAL);
+  dcu_build_info bi{};
+  int timed = 0;
+  // each build twice, the faster counts (the first may grow buffers)
+  auto build2 = [&](float* best) -> int {
+    float ms = 0.f;
+    for (int r = 0; r < 2; ++r) {
+      DCU_TRY(timed_build(c, n, nnz, ptr, idx, val, o, m, &bi, &ms));
+      *best = (r == 0 || ms < *best) ? ms : *best;
+    }
+    ++timed;
+    return DCU_OK;
+  };
+  DCU_TRY(build2(&t->build_ms_default));
+  t->build_ms_tuned = t->build_ms_default;
+  const int ncols = o.col_end - o.col_start;
+  if (bi.max_ni > 16 && ncols > 0) {
+    // |I_k| of every column, to skip limits that would hand more than 1/8 of
+    // the columns to the CTA kernel (a CTA per column costs more than a group
+    // of a warp by construction)
+    DCU_CUDA(c, cudaMalloc(&tmp->icount, sizeof(int) * (size_t)ncols));
+    DCU_CUDA(c, cudaMalloc(&tmp->iptr, sizeof(long long) * ((size_t)ncols + 1)));
+    long long total = 0;
+    DCU_TRY(dcu::spai_pattern(c, n, ptr, idx, o.col_start, o.col_end, tmp->icount, tmp->iptr, nullptr, 0, &total));
+    std::vector<int> h((size_t)ncols);
+    DCU_CUDA(c, cudaMemcpy(h.data(), tmp->icount, sizeof(int) * (size_t)ncols, cudaMemcpyDeviceToHost));
+    for (int v : {24, 16}) {
+      long long moved = 0;
+      for (int k : h) moved += (k > v && k <= 32) ? 1 : 0;
+      if (moved == 0 || moved > ncols / 8) continue;
+      c->tune[p].group_max_ni = v;
+      float ms = 0.f;
+      DCU_TRY(build2(&ms));
+      if (ms < 0.99f * t->build_ms_tuned) {
+        t->build_ms_tuned = ms;
+        t->group_max_ni = v;
+      }
+    }
+    c->tune[p].group_max_ni = t->group_max_ni;
+  }
+  // one solve from x0 = 0 with the chosen build and the default iteration
+  DCU_CUDA(c, cudaMalloc(&tmp->x, sizeof(double) * (size_t)n));
+  dcu_build_info b2{};
+  dcu_solve_info si{};
+  // best device time (ms) of the solve phase over three solves from x0 = 0
+  auto solve3 = [&](float* best) -> int {
+    for (int r = 0; r < 3; ++r) {
+      DCU_CUDA(c, cudaMemsetAsync(tmp->x, 0, sizeof(double) * (size_t)n, c->stream));
+      DCU_TRY(solve_pipeline(c, n, nnz, ptr, idx, val, b, tmp->x, o, nullptr, &b2, &si, nullptr, nullptr));
+      *best = (r == 0 || si.ms < *best) ? si.ms : *best;
+    }
+    ++timed;
+    return DCU_OK;
+  };
+  DCU_CUDA(c, cudaMemsetAsync(tmp->x, 0, sizeof(double) * (size_t)n, c->stream));
+  DCU_TRY(solve_pipeline(c, n, nnz, ptr, idx, val, b, tmp->x, o, nullptr, &b2, &si, nullptr, nullptr));
+  // per kernel: the fastest grid of each kernel without a reduction, single launches
+  dcu_tuning k = *t;
+  int it_timed = 0;
+  DCU_TRY(dcu::tune_iteration(c, reps, &k, &it_timed));
+  // Whole solves decide between the default, the per-kernel choice with the
+  // split and (where it computes the same values) with the fused first step:
+  // in a solve the kernels run inside a graph with programmatic dependent
+  // launch, where an extra launch costs less than it does alone.  Every
+  // candidate gives the same iterates, so the solve times compare launch
+  // configurations only.
+  const dcu_tuning base = c->tune[p];
+  std::vector<dcu_tuning> cands = {base};
+  auto add = [&](int k1) {
+    dcu_tuning v = base;
+    v.k1_split = k1;
+    v.grid_p = k.grid_p;
+    v.grid_y = k.grid_y;
+    v.grid_py = k.grid_py;
+    v.grid_sz = k.grid_sz;
+    const int eff = (k1 < 0) ? c->profile_default_split : k1;
+    const bool same = eff == c->profile_default_split && v.grid_sz == 0 &&
+                      (eff ? v.grid_p == 0 && v.grid_y == 0 : v.grid_py == 0);
+    if (!same) cands.push_back(v);
+  };
+  if (c->profile_k1_free) {
+    add(1);
+    add(0);
+  } else {
+    add(-1);
+  }
+  float def_ms = 0.f, best_ms = 0.f;
+  size_t pick = 0;
+  for (size_t i = 0; i < cands.size(); ++i) {
+    c->tune[p] = cands[i];
+    float ms = 0.f;
+    DCU_TRY(solve3(&ms));
+    if (i == 0) {
+      def_ms = best_ms = ms;
+    } else if (ms < 0.995f * best_ms) {  // a change must win by more than 0.5%
+      best_ms = ms;
+      pick = i;
+    }
+  }
+  const int iters = si.iters > 0 ? si.iters : 1;
+  t->k1_split = cands[pick].k1_split;
+  t->grid_p = cands[pick].grid_p;
+  t->grid_y = cands[pick].grid_y;
+  t->grid_py = cands[pick].grid_py;
+  t->grid_sz = cands[pick].grid_sz;
+  t->iter_us_default = 1000.f * def_ms / iters;
+  t->iter_us_tuned = 1000.f * best_ms / iters;
+  t->candidates = timed + it_timed;
+  c->tune[p] = *t;
+  return DCU_OK;
+}
+
+int check_tuning(Ctx* c, const dcu_tuning* t) {
+  if (t->k1_split < -1 || t->k1_split > 1) return dcu::fail(c, DCU_ERR_ARG, "k1_split must be -1, 0 or 1");
+  for (int g : {t->grid_p, t->grid_y, t->grid_py, t->grid_sz})
+    if (g < -1 || g > 64) return dcu::fail(c, DCU_ERR_ARG, "grid selector %d outside [-1, 64]", g);
+  if (t->group_max_ni < 0 || t->group_max_ni > 32)
+    return dcu::fail(c, DCU_ERR_ARG, "group_max_ni %d outside [0, 32]", t->group_max_ni);
+  return DCU_OK;
+}
+
 }  // namespace
 
 extern "C" {
+
+void dcu_tuning_default(dcu_tuning* t) {
+  if (!t) return;
+  std::memset(t, 0, sizeof(*t));
+  t->k1_split = -1;
+}
+
+int dcu_set_tuning(dcu_spai_ctx* c, int precision, const dcu_tuning* t) {
+  if (!c) return DCU_ERR_ARG;
+  if (precision < DCU_PREC_FP64 || precision > DCU_PREC_M_BF16)
+    return dcu::fail(c, DCU_ERR_ARG, "unknown precision %d", precision);
+  if (!t) {
+    dcu_tuning_default(&c->tune[precision]);
+    c->tune_set[precision] = false;
+    return DCU_OK;
+  }
+  DCU_TRY(check_tuning(c, t));
+  c->tune[precision] = *t;
+  c->tune_set[precision] = true;
+  return DCU_OK;
+}
+
+int dcu_get_tuning(dcu_spai_ctx* c, int precision, dcu_tuning* t) {
+  if (!c || !t) return DCU_ERR_ARG;
+  if (precision < DCU_PREC_FP64 || precision > DCU_PREC_M_BF16)
+    return dcu::fail(c, DCU_ERR_ARG, "unknown precision %d", precision);
+  if (c->tune_set[precision]) *t = c->tune[precision];
+  else dcu_tuning_default(t);
+  return DCU_OK;
+}
+
+int dcu_autotune_d(dcu_spai_ctx* c, int n, int nnz, const int* ptr, const int* idx, const double* val,
+                   const double* b, const dcu_options* opt, int reps, dcu_tuning* out) {
+  int rc = check_matrix(c, n, nnz, ptr, idx, val);
+  if (rc) return rc;
+  if (!b) return dcu::fail(c, DCU_ERR_ARG, "null vector");
+  dcu_options o;
+  if ((rc = resolve_range(c, n, opt, &o))) return rc;
+  const int p = o.precision;
+  const bool was_set = c->tune_set[p];
+  const dcu_tuning was = c->tune[p];
+  dcu_tuning t;
+  TuneScratch tmp;
+  try {
+    StreamScope scope(c);
+    rc = autotune(c, n, nnz, ptr, idx, val, b, o, reps, &t, &tmp);
+    cudaStreamSynchronize(c->stream);
+  } catch (const std::bad_alloc&) {
+    rc = dcu::fail(c, DCU_ERR_ALLOC, "host allocation failed");
+  }
+  cudaFree(tmp.x);
+  cudaFree(tmp.icount);
+  cudaFree(tmp.iptr);
+  if (rc) {
+    c->tune[p] = was;
+    c->tune_set[p] = was_set;
+    return rc;
+  }
+  c->tune[p] = t;
+  c->tune_set[p] = true;
+  if (out) *out = t;
+  return DCU_OK;
+}
 
 void dcu_options_default(dcu_options* o) {
   if (!o) return;

@@ -91,11 +91,22 @@ struct Ctx {
   void* pinned = nullptr;   // small pinned host scratch (flags, stats), kPinnedBytes
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   std::vector<GraphSlot> graphs;  // BiCGSTAB iteration graphs (bounded cache)
-  // launches iteration kernel j (0..4) of the last solve on its buffers, with
-  // the solver's stop flag cleared first (diagnostic timing only)
-  std::function<int(int)> profile_launch;
-  int profile_kernels = 0;
+  // launch configuration per precision form (dcu_set_tuning / dcu_autotune_d)
+  dcu_tuning tune[5];
+  bool tune_set[5] = {false, false, false, false, false};
+  // launches iteration kernel `kind` (IterKernel) of the last solve on its
+  // buffers with grid selector `sel`, the solver's stop flag cleared first
+  // (diagnostic timing and the autotuner only)
+  std::function<int(int kind, int sel)> profile_launch;
+  std::function<int(int kind, int sel)> profile_grid;  // the grid that launch uses
+  std::vector<int> profile_order;  // kinds in the last solve's launch order
+  std::vector<int> profile_sel;    // and the grid selector each ran with
+  bool profile_k1_free = false;    // fused and split first steps compute the same values
+  int profile_default_split = 0;   // the form's default first step
 };
+
+// Iteration kernels of BiCGSTAB, for profiling and the autotuner.
+enum IterKernel { IK_P = 0, IK_Y, IK_PY, IK_AY, IK_SZ, IK_AZ, IK_XR, IK_COUNT };
 
 constexpr size_t kPinnedBytes = 4096;
 
@@ -196,6 +207,11 @@ int batch_solve(Ctx* c, int nsys, const int* sys_off, const SellPlan& plan, cons
                 int nrhs, const double* B, double* X, const dcu_options* opt, int* iters, int* status,
                 dcu_solve_info* info);
 int profile_iteration(Ctx* c, int reps, float* ms, int cap, int* count);
+// Times the grid selectors of the kernels without a reduction (and the fused
+// against the split first step where both compute the same values) on the
+// last solve's buffers; writes the fastest into t's iteration fields and the
+// report's iteration times.
+int tune_iteration(Ctx* c, int reps, dcu_tuning* t, int* timed);
 
 // grid size for grid-stride kernels: whole waves of `per_sm` blocks
 inline int waves_grid(const Ctx* c, long long work_items, int block, int per_sm) {

@@ -13,7 +13,8 @@
 //
 // Two kernels share the column range through a device work queue:
 //   k_spai_small  one 8-lane group per column, |J_k| <= 7, <= 64 candidate
-//                 rows, |I_k| <= 32: candidates sorted in registers (bitonic
+//                 rows, |I_k| <= 32 (or the tuned group_max_ni below it):
+//                 candidates sorted in registers (bitonic
 //                 network across the group), At staged in shared memory, one
 //                 lane per column of [At | e_E] holding it in registers.
 //   k_spai_large  one CTA per column for everything else: I_k by a bitmap
@@ -82,6 +83,7 @@ struct SmallArgs {
   int* big_list;
   int* stats;
   const int* list;    // when set: process these columns (count in stats[ST_FB_COUNT])
+  int max_ni;         // largest |I_k| this kernel takes (<= SG_MMAX); larger go to the CTA kernel
 };
 
 // Shared state of the two groups of a warp.  Row strides are padded so the
@@ -279,7 +281,7 @@ __device__ __forceinline__ int group_column(const SmallArgs& a, WarpSmem<T>& ws,
   const int excl = inc - cnt;
   const int m = __shfl_sync(gmask, inc, GL - 1, GL);
 
-  if (m > SG_MMAX) {
+  if (m > a.max_ni) {
     if (lane == 0) queue_big(a, k, nj, (long long)cand * (nj + 1));
     return -1;
   }
@@ -1207,6 +1209,7 @@ int prepare(Ctx* c, int n, const int* ptr, const int* idx, const double* val, in
   a.big_list = bp<int>(c, B_BIGLIST);
   a.stats = stats;
   a.units = c->units;
+  a.max_ni = SG_MMAX;
   P->stats = stats;
   return DCU_OK;
 }
@@ -1221,9 +1224,10 @@ int read_stats(Ctx* c, int* host) {
 
 template <typename T>
 int build_typed(Ctx* c, int n, const int* ptr, const int* idx, const double* val, int col_start, int col_end,
-                int schedule, bool thread_path, double* mval, double* colres, dcu_build_info* info) {
+                int schedule, bool thread_path, int max_ni, double* mval, double* colres, dcu_build_info* info) {
   Prepared P;
   DCU_TRY(prepare(c, n, ptr, idx, val, col_start, col_end, schedule, &P));
+  if (max_ni > 0 && max_ni < SG_MMAX) P.sa.max_ni = max_ni;
   P.sa.mval = mval;
   P.sa.colres = colres;
   int st[ST_INTS];
@@ -1308,14 +1312,16 @@ int spai_build(Ctx* c, int n, int nnz, const int* ptr, const int* idx, const dou
   if (col_start != 0 || col_end != n)
     DCU_CUDA(c, cudaMemsetAsync(mval, 0, sizeof(double) * (size_t)(nnz > 0 ? nnz : 1), c->stream));
   if (col_end <= col_start) return DCU_OK;
+  const int p = opt->precision;
+  const int max_ni = (p >= 0 && p < 5 && c->tune_set[p]) ? c->tune[p].group_max_ni : 0;
   // FP64 (the plain form): Householder on every column unless the normal
   // equations are asked for.  Mixed forms: the thread-per-column path first,
   // Householder for the columns it hands over, unless Householder is asked for.
   if (opt->precision == DCU_PREC_FP64)
     return build_typed<double>(c, n, ptr, idx, val, col_start, col_end, opt->schedule,
-                               opt->ls_method == DCU_LS_NORMAL_EQ, mval, colres, info);
+                               opt->ls_method == DCU_LS_NORMAL_EQ, max_ni, mval, colres, info);
   return build_typed<float>(c, n, ptr, idx, val, col_start, col_end, opt->schedule, opt->ls_method != DCU_LS_HOUSEHOLDER,
-                            mval, colres, info);
+                            max_ni, mval, colres, info);
 }
 
 int spai_pattern(Ctx* c, int n, const int* ptr, const int* idx, int col_start, int col_end, int* icount,

@@ -43,6 +43,19 @@ class SolveInfo(C.Structure):
                 ("true_res", C.c_double), ("bnorm", C.c_double), ("ms", C.c_float)]
 
 
+class Tuning(C.Structure):
+    """dcu_tuning: launch configuration of one precision form and the autotuner's report."""
+    _fields_ = [("k1_split", C.c_int), ("grid_p", C.c_int), ("grid_y", C.c_int), ("grid_py", C.c_int),
+                ("grid_sz", C.c_int), ("group_max_ni", C.c_int), ("iter_us_default", C.c_float),
+                ("iter_us_tuned", C.c_float), ("build_ms_default", C.c_float), ("build_ms_tuned", C.c_float),
+                ("candidates", C.c_int)]
+
+    CONFIG = ("k1_split", "grid_p", "grid_y", "grid_py", "grid_sz", "group_max_ni")
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 _LIB = None
 _vp = C.c_void_p
 _i = C.c_int
@@ -75,6 +88,10 @@ SIGNATURES = {
                                C.POINTER(BuildInfo), C.POINTER(SolveInfo)]),
     "dcu_profile_iteration_kernels": (_i, [_vp, _i, C.POINTER(C.c_float), _i, C.POINTER(_i)]),
     "dcu_sell_plan_stats": (_i, [_vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
+    "dcu_tuning_default": (None, [C.POINTER(Tuning)]),
+    "dcu_set_tuning": (_i, [_vp, _i, C.POINTER(Tuning)]),
+    "dcu_get_tuning": (_i, [_vp, _i, C.POINTER(Tuning)]),
+    "dcu_autotune_d": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, _OPT, _i, C.POINTER(Tuning)]),
     "dcu_mtx_read": (_i, [C.c_char_p, C.POINTER(_i), C.POINTER(_i), C.POINTER(C.POINTER(_i)),
                           C.POINTER(C.POINTER(_i)), C.POINTER(C.POINTER(C.c_double))]),
     "dcu_mtx_free": (None, [_vp]),

@@ -132,7 +132,7 @@ typedef struct {
   int ls_method;          /* dcu_ls_method                                  */
 } dcu_options;
 
-/* Fill *opt with the defaults of the BASELINE configs: balanced_columns,
+/* Fill *opt with the defaults of the benchmark workloads: balanced_columns,
  * FP64, relative tol 1e-8, maxiter 1000, verify on, all columns. */
 void dcu_options_default(dcu_options* opt);
 
@@ -282,6 +282,63 @@ int dcu_profile_iteration_kernels(dcu_spai_ctx* ctx, int reps, float* ms_out, in
  * 32 rows (those slices read no index array).  Either output may be NULL.
  * No counterpart in the reference. */
 int dcu_sell_plan_stats(dcu_spai_ctx* ctx, long long* slots, long long* uniform_slots);
+
+/* ---- autotuner (no counterpart in the reference) ----------------------------- */
+
+/* Launch configuration of one precision form.  Grid selectors: 0 = one wave
+ * of as many blocks as fit on the GPU at once (each thread loops over rows),
+ * -1 = one block per 256 rows (row pairs for the p pass: no loop), k > 0 =
+ * k blocks per SM (capped at what fits).  A row's arithmetic does not depend
+ * on the grid, and the two first steps compute the same values, so every
+ * field except group_max_ni leaves the solution bit-identical:
+ *   k1_split   -1: the form's default (split with an FP32 / BF16 M, fused
+ *              with an FP64 M); 0: fused (p formed at every gathered column
+ *              inside y = M p); 1: split (a p pass, then y = M p).  Forms with
+ *              FP32 vectors keep their default: their fused step multiplies
+ *              by the unrounded p, so the two differ in rounding there.
+ *   grid_p, grid_y, grid_py, grid_sz   the kernels without a reduction:
+ *              p pass, y = M p, fused p/y, s/z = M s.  The kernels that end
+ *              in a dot product keep one full wave: their grid fixes the
+ *              summation order of the partial sums.
+ *   group_max_ni   SPAI build: largest |I_k| the warp-group (warp-per-small)
+ *              kernel takes, 1..32 (0 = 32); larger columns go to the
+ *              CTA-per-column kernel.  Changes M by rounding only.
+ * The report fields are written by dcu_autotune_d and ignored on input. */
+typedef struct {
+  int k1_split;
+  int grid_p, grid_y, grid_py, grid_sz;
+  int group_max_ni;
+  /* report */
+  float iter_us_default;  /* solve ms / iterations with the default iteration configuration      */
+  float iter_us_tuned;    /* the same with the chosen one                                         */
+  float build_ms_default; /* SPAI build with group_max_ni = 32                                   */
+  float build_ms_tuned;   /* SPAI build with the chosen group_max_ni                             */
+  int candidates;         /* launch configurations timed                                         */
+} dcu_tuning;
+
+/* Defaults: every selector 0, k1_split -1, group_max_ni 0, report zero. */
+void dcu_tuning_default(dcu_tuning* t);
+
+/* Use *t for every later build and solve of `precision` on this context
+ * (NULL: back to the defaults).  DCU_ERR_ARG on a selector out of range. */
+int dcu_set_tuning(dcu_spai_ctx* ctx, int precision, const dcu_tuning* t);
+int dcu_get_tuning(dcu_spai_ctx* ctx, int precision, dcu_tuning* t);
+
+/* Time the candidate configurations of opt->precision on this matrix and
+ * keep the fastest (as dcu_set_tuning would).  Steps: (1) two builds per
+ * group_max_ni candidate (32, 24, 16; a candidate that would hand more than
+ * 1/8 of the columns to the CTA kernel is not timed); (2) one solve of
+ * A x = b from x0 = 0 with the chosen build, then each kernel without a
+ * reduction at grid selectors 0, -1 and half the resident blocks, `reps`
+ * single launches each (<= 0: 10), every timed launch right after an untimed
+ * launch of its predecessor in the iteration; (3) three whole solves each of
+ * the default, the per-kernel choice with the split and (FP64 vectors) with
+ * the fused first step: the fastest solve phase wins, a change by more than
+ * 0.5%.  Every candidate of (2)-(3) gives the same iterates, so solve times
+ * compare launch configurations only.  Device arrays; b is not modified.
+ * *out (optional) receives the choice and the report. */
+int dcu_autotune_d(dcu_spai_ctx* ctx, int n, int nnz, const int* ptr, const int* idx, const double* val,
+                   const double* b, const dcu_options* opt, int reps, dcu_tuning* out);
 
 /* ---- MatrixMarket input (command-line driver) --------------------------------- */
 
