@@ -271,10 +271,12 @@ __global__ void __launch_bounds__(BI_BLOCK) k_bi_py(BiArgs<MT, IT, VT> a) {
 // Split form of K1, used with a narrow (FP32 / BF16) preconditioner: p is
 // formed once per row by a streaming kernel and then read by a one-vector
 // SpMV, instead of at every gathered column (three gathered vectors per
-// entry).  Same arithmetic as the fused kernel.  With an FP64 M the SpMV
-// itself moves 8 bytes of value per entry and the extra launch and pass cost
-// more than the gathers they save, so K1 stays fused there; K3 gathers two
-// vectors and stays fused always.
+// entry).  Same arithmetic as the fused kernel.  This is the untuned default:
+// split with a narrow M, fused with an FP64 M (whose SpMV moves 8 bytes of
+// value per entry, so the gathers the split saves weigh less).  The autotuner
+// compares both in whole solves where they compute the same values (FP64
+// vectors); at 128^3 it finds the split faster with an FP64 M too.  K3
+// gathers two vectors and stays fused always.
 template <typename MT>
 constexpr bool split_k1() {
   return !std::is_same<MT, double>::value;
