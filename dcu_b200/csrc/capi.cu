@@ -215,6 +215,17 @@ int autotune(Ctx* c, int n, int nnz, const int* ptr, const int* idx, const doubl
     }
     c->tune[p].group_max_ni = t->group_max_ni;
   }
+  if (bi.cols_hub > 0) {
+    // every block on one CTA (per-CTA slabs) against the hub kernels
+    c->tune[p].cta_max_area = -1;
+    float ms = 0.f;
+    DCU_TRY(build2(&ms));
+    if (ms < 0.99f * t->build_ms_tuned) {
+      t->build_ms_tuned = ms;
+      t->cta_max_area = -1;
+    }
+    c->tune[p].cta_max_area = t->cta_max_area;
+  }
   // one solve from x0 = 0 with the chosen build and the default iteration
   DCU_CUDA(c, cudaMalloc(&tmp->x, sizeof(double) * (size_t)n));
   dcu_build_info b2{};
@@ -293,6 +304,7 @@ int check_tuning(Ctx* c, const dcu_tuning* t) {
     if (g < -1 || g > 64) return dcu::fail(c, DCU_ERR_ARG, "grid selector %d outside [-1, 64]", g);
   if (t->group_max_ni < 0 || t->group_max_ni > 32)
     return dcu::fail(c, DCU_ERR_ARG, "group_max_ni %d outside [0, 32]", t->group_max_ni);
+  if (t->cta_max_area < -1) return dcu::fail(c, DCU_ERR_ARG, "cta_max_area must be >= -1");
   return DCU_OK;
 }
 

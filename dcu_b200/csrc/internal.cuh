@@ -52,6 +52,9 @@ enum BufId {
   B_SORTTMP,       // global scratch of the long-row sort
   B_FBLIST,        // columns handed from the thread kernel to the group kernel
   B_PLANSTAT,      // slots of the last SELL plan in offset-uniform slices
+  B_HUBPOOL,       // slabs of the columns factored by the hub kernels
+  B_HUBMETA,       // their descriptors
+  B_HUBWPRE,       // prefix of their widths (warp -> column map)
   B_COUNT
 };
 

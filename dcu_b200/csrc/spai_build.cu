@@ -25,7 +25,9 @@
 // kernel drains with an atomic counter.  Each column's arithmetic is fixed by
 // its own data (fixed reduction trees, no float atomics), so M is identical
 // for every schedule and grid size.
+#include <algorithm>
 #include <climits>
+#include <vector>
 
 #include "internal.cuh"
 
@@ -51,8 +53,11 @@ enum {
   ST_NE_COLS = 12,    // columns finished by the thread kernel
   ST_STAGE_FAIL = 13, // a bulk copy into shared memory did not complete in time
   ST_STAGED = 16,     // CTA-kernel columns whose J columns were staged by bulk copies
+  ST_HUB_COUNT = 17,  // columns handed to the hub kernels
   ST_INTS = 24,
-  ST_AREA64 = 7       // long long index (ints 14-15): max candidates * (|J|+1) over queued columns
+  ST_AREA64 = 7,      // long long index (ints 14-15): max candidates * (|J|+1) over queued columns
+  ST_AREASUM64 = 9,   // long long index (ints 18-19): sum of (candidates + 2) * (|J|+1) over queued columns
+  ST_HUBHEAD64 = 10   // long long index (ints 20-21): elements of the hub pool handed out
 };
 
 constexpr int GL = 16;          // lanes per least-squares problem: 2 per column of [At | e_E]
@@ -104,6 +109,8 @@ __device__ __forceinline__ void queue_big(const SmallArgs& a, int k, int nj, lon
   a.big_list[q] = k;
   atomicMax(&a.stats[ST_BIG_MAXNJ], nj);
   atomicMax(reinterpret_cast<unsigned long long*>(a.stats) + ST_AREA64, (unsigned long long)area);
+  // bound of the column's hub slab: |I| (<= candidates) x (|J| + 1), plus two scalars per step
+  atomicAdd(reinterpret_cast<unsigned long long*>(a.stats) + ST_AREASUM64, (unsigned long long)(area + 2LL * (nj + 1)));
 }
 
 // Bitonic sort of GL*PER keys held PER per lane (element e = lane*PER + s),
@@ -687,6 +694,15 @@ constexpr int LG_WORDS_SMEM = 4096;  // bitmap words kept in shared memory
 constexpr int LG_STAGE_NJ = 256;     // J columns staged in shared memory by bulk copies
 constexpr int LG_STAGE_BYTES = 48 * 1024;
 constexpr long long kStageWaitSpins = 1ll << 22;
+constexpr long long kHubPoolMax = 1ll << 28;  // elements of the hub pool (2 GB in FP64)
+
+// A column factored by the hub kernels: its dense block [A(I,J) | e_E]
+// (m x (nj+1), column-major) at pool + off, followed by the Householder
+// scalars alpha (R's diagonal) and beta of each step, (nj+1) each.
+struct HubMeta {
+  int k, m, nj, pad;
+  long long off;
+};
 
 struct LargeArgs {
   int n;
@@ -707,6 +723,11 @@ struct LargeArgs {
   long long area_per_block;
   long long smem_area;     // elements of T that fit the shared slab
   int stage_ok;            // idx (and val when building) 16-byte aligned: bulk copies allowed
+  long long area_sum;      // ST_AREASUM64 of the queue (host side)
+  long long hub_min_area;  // blocks larger than this go to the hub pool
+  void* hub_pool;          // build: slabs of columns whose block exceeds shared memory (T)
+  long long hub_cap;       // elements of T in hub_pool
+  HubMeta* hub_meta;       // one per hub column, in hand-off order
 };
 
 // Bulk copies (the TMA engine, no multicast) of global ranges into this CTA's
@@ -759,6 +780,7 @@ struct LargeSmem {
   int jso[LG_STAGE_NJ + 1];  // staged int range of J column j starts at jso[j] ints
   int jvo[LG_STAGE_NJ + 1];  // staged double range of J column j starts at jvo[j] doubles
   unsigned long long mbar;   // completion of the bulk copies
+  long long hub_off;
   int col_q;
   int m;
   int E;
@@ -1000,7 +1022,25 @@ __global__ void __launch_bounds__(LG_BLOCK, 1) k_spai_large(LargeArgs a) {
     const long long lda = m;
     const long long area = (long long)m * W;
     T* Ad = (area <= a.smem_area) ? sA : gA;
-    if (area > a.smem_area && area > a.area_per_block) {
+    // A block that does not fit shared memory is gathered into its own slab
+    // of the hub pool and factored by the hub kernels (all SMs on all such
+    // columns, one launch per Householder step) instead of by this CTA alone.
+    bool hub = false;
+    if (area > a.hub_min_area && a.hub_pool) {
+      if (tid == 0) {
+        const long long need = area + 2LL * W;
+        const long long off = (long long)atomicAdd(reinterpret_cast<unsigned long long*>(a.stats) + ST_HUBHEAD64,
+                                                   (unsigned long long)need);
+        S.hub_off = (off + need <= a.hub_cap) ? off : -1;
+        if (S.hub_off >= 0) a.hub_meta[atomicAdd(&a.stats[ST_HUB_COUNT], 1)] = HubMeta{k, m, nj, 0, off};
+      }
+      __syncthreads();
+      if (S.hub_off >= 0) {
+        Ad = reinterpret_cast<T*>(a.hub_pool) + S.hub_off;
+        hub = true;
+      }
+    }
+    if (!hub && area > a.smem_area && area > a.area_per_block) {
       if (tid == 0) atomicAdd(&a.stats[ST_LIMIT], 1);
       continue;
     }
@@ -1026,6 +1066,7 @@ __global__ void __launch_bounds__(LG_BLOCK, 1) k_spai_large(LargeArgs a) {
     }
     if (tid == 0 && S.E >= 0) Ad[(long long)nj * lda + S.E] = T(1);
     __syncthreads();
+    if (hub) continue;  // factored, solved and scattered by the hub kernels
     bool sing = m < nj;
     const int steps = min(nj, m);
     for (int c = 0; c < steps; ++c) {
@@ -1075,7 +1116,8 @@ __global__ void __launch_bounds__(LG_BLOCK, 1) k_spai_large(LargeArgs a) {
       }
       __syncthreads();
       const T xi = S.ys[i];
-      for (int t = tid; t < i; t += LG_BLOCK) S.ys[t] -= Ad[(long long)i * lda + t] * xi;
+      // R has min(m, nj) rows: column i holds R(t, i) for t < min(i, m)
+      for (int t = tid; t < min(i, m); t += LG_BLOCK) S.ys[t] -= Ad[(long long)i * lda + t] * xi;
       __syncthreads();
     }
     for (int t = tid; t < nj; t += LG_BLOCK) a.mval[cs + t] = (double)S.ys[t];
@@ -1086,6 +1128,114 @@ __global__ void __launch_bounds__(LG_BLOCK, 1) k_spai_large(LargeArgs a) {
       atomicAdd(&a.stats[ST_BIG_DONE], 1);
     }
     __syncthreads();
+  }
+}
+
+// ---- hub kernels: columns whose dense block exceeds shared memory ---------
+// One launch per Householder step c, over every hub column at once: a warp
+// per trailing column j > c applies reflector c (the dot product and update
+// of the CTA kernel, lanes striding the rows), and the warp of column c + 1
+// then forms reflector c + 1 from its updated column.  Launch c = -1 forms
+// reflector 0.  Each hub's block streams through L2 on all SMs instead of
+// through one SM.  k_hub_solve then back-substitutes, one CTA per column.
+constexpr int HUB_BLOCK = 256;
+
+struct HubArgs {
+  const HubMeta* meta;
+  const int* wpre;  // wpre[h] = sum of (nj + 1) over hubs before h; warp w works in hub h when wpre[h] <= w
+  int nh;
+  int total_w;      // wpre[nh]
+  void* pool;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(HUB_BLOCK) k_hub_step(HubArgs h, int c) {
+  const int gw = (int)(((long long)blockIdx.x * HUB_BLOCK + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (gw >= h.total_w) return;
+  int lo = 0, hi = h.nh - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (h.wpre[mid] <= gw) lo = mid;
+    else hi = mid - 1;
+  }
+  const HubMeta hm = h.meta[lo];
+  const int W = hm.nj + 1;
+  const int j = c + 1 + (gw - h.wpre[lo]);
+  if (j >= W) return;
+  const int m = hm.m;
+  const int steps = min(hm.nj, m);
+  T* Ad = reinterpret_cast<T*>(h.pool) + hm.off;
+  T* rd = Ad + (long long)m * W;
+  T* bt = rd + W;
+  T* aj = Ad + (long long)j * m;
+  if (c >= 0 && c < steps) {
+    const T beta = bt[c];
+    if (beta != T(0)) {
+      const T* vc = Ad + (long long)c * m;
+      T w = T(0);
+      for (int i = c + lane; i < m; i += 32) w += vc[i] * aj[i];
+#pragma unroll
+      for (int d = 16; d > 0; d >>= 1) w += __shfl_xor_sync(0xffffffffu, w, d);
+      w *= beta;
+      for (int i = c + lane; i < m; i += 32) aj[i] -= w * vc[i];
+    }
+  }
+  if (j == c + 1 && j < steps) {
+    double part = 0.0;
+    for (int i = j + lane; i < m; i += 32) part += (double)aj[i] * (double)aj[i];
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) part += __shfl_xor_sync(0xffffffffu, part, d);
+    __syncwarp();  // aj[j] was updated by another lane
+    if (lane == 0) {
+      const T x0 = aj[j];
+      const T nrm = (T)sqrt(part);
+      T alpha = T(0), beta = T(0);
+      if (nrm > T(0)) {
+        alpha = (x0 > T(0)) ? -nrm : nrm;
+        beta = T(1) / (nrm * (nrm + (T)fabs((double)x0)));
+        aj[j] = x0 - alpha;
+      }
+      rd[j] = alpha;
+      bt[j] = beta;
+    }
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(LG_BLOCK) k_hub_solve(HubArgs h, LargeArgs a) {
+  __shared__ T ys[LG_NJ_MAX];
+  __shared__ double red[LG_WARPS];
+  const HubMeta hm = h.meta[blockIdx.x];
+  const int tid = threadIdx.x;
+  const int m = hm.m, nj = hm.nj, W = nj + 1;
+  const T* Ad = reinterpret_cast<const T*>(h.pool) + hm.off;
+  const T* rd = Ad + (long long)m * W;
+  const T* y = Ad + (long long)nj * m;
+  for (int t = tid; t < nj; t += LG_BLOCK) ys[t] = (t < m) ? y[t] : T(0);
+  double part = 0.0;
+  for (int i = nj + tid; i < m; i += LG_BLOCK) part += (double)y[i] * (double)y[i];
+  const double res2 = block_sum(part, red);
+  __syncthreads();
+  bool sing = m < nj;
+  for (int i = nj - 1; i >= 0; --i) {
+    if (tid == 0) {
+      const T rii = (i < m) ? rd[i] : T(0);
+      if (!(rii != T(0)) || !isfinite((double)rii)) sing = true;
+      ys[i] = ys[i] / rii;
+    }
+    __syncthreads();
+    const T xi = ys[i];
+    for (int t = tid; t < min(i, m); t += LG_BLOCK) ys[t] -= Ad[(long long)i * m + t] * xi;
+    __syncthreads();
+  }
+  const int cs = a.ptr[hm.k];
+  for (int t = tid; t < nj; t += LG_BLOCK) a.mval[cs + t] = (double)ys[t];
+  if (tid == 0) {
+    if (a.colres) a.colres[hm.k - a.col_start] = sqrt(res2);
+    if (sing) atomicAdd(&a.stats[ST_SINGULAR], 1);
+    atomicMax(&a.stats[ST_MAXNI], m);
+    atomicAdd(&a.stats[ST_BIG_DONE], 1);
   }
 }
 
@@ -1134,7 +1284,7 @@ int run_small(Ctx* c, SmallArgs a, int) {
 }
 
 template <typename T, int MODE>
-int run_large(Ctx* c, LargeArgs& a, int nbig) {
+int run_large(Ctx* c, LargeArgs& a, int nbig, int cta_max_area = 0) {
   const size_t fixed = ((sizeof(LargeSmem<T>) + 15) / 16) * 16 + LG_STAGE_BYTES;
   size_t cap = c->smem_optin > fixed + 1024 ? c->smem_optin - 1024 : fixed;
   // bulk copies read idx (every mode) and val (build only) in 16-byte units
@@ -1148,12 +1298,56 @@ int run_large(Ctx* c, LargeArgs& a, int nbig) {
   a.words_per_block = ((long long)a.n >> 5) + 2;
   const long long area_cap = a.area_per_block;
   a.area_per_block = (MODE == MODE_BUILD && area_cap > a.smem_area) ? area_cap : 0;
+  // Blocks that exceed shared memory go to the hub pool, sized by the queue's
+  // bound; the per-CTA slabs remain only for what a capped pool cannot hold.
+  a.hub_pool = nullptr;
+  a.hub_cap = 0;
+  a.hub_meta = nullptr;
+  a.hub_min_area = a.smem_area > cta_max_area ? a.smem_area : cta_max_area;
+  if (MODE == MODE_BUILD && a.area_per_block > a.hub_min_area && cta_max_area >= 0) {
+    a.hub_cap = a.area_sum < kHubPoolMax ? a.area_sum : kHubPoolMax;
+    DCU_TRY(ensure(c, B_HUBPOOL, sizeof(T) * (size_t)a.hub_cap));
+    DCU_TRY(ensure(c, B_HUBMETA, sizeof(HubMeta) * (size_t)nbig));
+    a.hub_pool = c->buf[B_HUBPOOL].p;
+    a.hub_meta = bp<HubMeta>(c, B_HUBMETA);
+    // the pool holds every block above shared memory: no per-CTA slabs
+    if (a.hub_cap == a.area_sum && a.hub_min_area == a.smem_area) a.area_per_block = 0;
+  }
   DCU_TRY(ensure(c, B_SLAB_BITS, sizeof(unsigned) * 2 * (size_t)a.words_per_block * grid));
   a.gbits = bp<unsigned>(c, B_SLAB_BITS);
   if (a.area_per_block > 0) DCU_TRY(ensure(c, B_SLAB_A, sizeof(T) * (size_t)a.area_per_block * grid));
   a.gA = a.area_per_block > 0 ? c->buf[B_SLAB_A].p : nullptr;
   k_spai_large<T, MODE><<<grid, LG_BLOCK, smem, c->stream>>>(a);
   DCU_LAUNCHED(c, "k_spai_large");
+  if (!a.hub_pool) return DCU_OK;
+  // hub columns: read their descriptors, map warps to (column, trailing
+  // column), one step launch per Householder step, then the solves
+  int* st = bp<int>(c, B_STATS);
+  DCU_CUDA(c, cudaMemcpyAsync(c->pinned, st + ST_HUB_COUNT, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  DCU_CUDA(c, cudaStreamSynchronize(c->stream));
+  const int nh = *reinterpret_cast<int*>(c->pinned);
+  if (nh <= 0) return DCU_OK;
+  std::vector<HubMeta> hm((size_t)nh);
+  DCU_CUDA(c, cudaMemcpyAsync(hm.data(), a.hub_meta, sizeof(HubMeta) * (size_t)nh, cudaMemcpyDeviceToHost,
+                              c->stream));
+  DCU_CUDA(c, cudaStreamSynchronize(c->stream));
+  std::vector<int> wpre((size_t)nh + 1, 0);
+  int steps = 0;
+  for (int h = 0; h < nh; ++h) {
+    wpre[h + 1] = wpre[h] + hm[h].nj + 1;
+    steps = std::max(steps, std::min(hm[h].nj, hm[h].m));
+  }
+  DCU_TRY(ensure(c, B_HUBWPRE, sizeof(int) * wpre.size()));
+  DCU_CUDA(c, cudaMemcpyAsync(c->buf[B_HUBWPRE].p, wpre.data(), sizeof(int) * wpre.size(), cudaMemcpyHostToDevice,
+                              c->stream));
+  HubArgs h{a.hub_meta, bp<int>(c, B_HUBWPRE), nh, wpre[nh], a.hub_pool};
+  const int blocks = (int)(((long long)wpre[nh] * 32 + HUB_BLOCK - 1) / HUB_BLOCK);
+  for (int cst = -1; cst < steps; ++cst) {
+    k_hub_step<T><<<blocks, HUB_BLOCK, 0, c->stream>>>(h, cst);
+    DCU_LAUNCHED(c, "k_hub_step");
+  }
+  k_hub_solve<T><<<nh, LG_BLOCK, 0, c->stream>>>(h, a);
+  DCU_LAUNCHED(c, "k_hub_solve");
   return DCU_OK;
 }
 
@@ -1224,7 +1418,8 @@ int read_stats(Ctx* c, int* host) {
 
 template <typename T>
 int build_typed(Ctx* c, int n, const int* ptr, const int* idx, const double* val, int col_start, int col_end,
-                int schedule, bool thread_path, int max_ni, double* mval, double* colres, dcu_build_info* info) {
+                int schedule, bool thread_path, int max_ni, int cta_max_area, double* mval, double* colres,
+                dcu_build_info* info) {
   Prepared P;
   DCU_TRY(prepare(c, n, ptr, idx, val, col_start, col_end, schedule, &P));
   if (max_ni > 0 && max_ni < SG_MMAX) P.sa.max_ni = max_ni;
@@ -1275,7 +1470,8 @@ int build_typed(Ctx* c, int n, const int* ptr, const int* idx, const double* val
     long long area = 0;
     memcpy(&area, reinterpret_cast<long long*>(st) + ST_AREA64, sizeof area);
     la.area_per_block = area;
-    DCU_TRY((run_large<T, MODE_BUILD>(c, la, nbig)));
+    memcpy(&la.area_sum, reinterpret_cast<long long*>(st) + ST_AREASUM64, sizeof la.area_sum);
+    DCU_TRY((run_large<T, MODE_BUILD>(c, la, nbig, cta_max_area)));
     DCU_TRY(read_stats(c, st));
     if (st[ST_LIMIT] > 0) return fail(c, DCU_ERR_LIMIT, "%d columns exceeded the CTA kernel's limits", st[ST_LIMIT]);
     if (st[ST_STAGE_FAIL] > 0) return fail(c, DCU_ERR_CUDA, "a bulk copy into shared memory did not complete");
@@ -1288,6 +1484,7 @@ int build_typed(Ctx* c, int n, const int* ptr, const int* idx, const double* val
     info->max_nj = st[ST_MAXNJ] > st[ST_BIG_MAXNJ] ? st[ST_MAXNJ] : st[ST_BIG_MAXNJ];
     info->max_ni = st[ST_MAXNI];
     info->cols_staged = st[ST_STAGED];
+    info->cols_hub = st[ST_HUB_COUNT];
   }
   return DCU_OK;
 }
@@ -1313,15 +1510,17 @@ int spai_build(Ctx* c, int n, int nnz, const int* ptr, const int* idx, const dou
     DCU_CUDA(c, cudaMemsetAsync(mval, 0, sizeof(double) * (size_t)(nnz > 0 ? nnz : 1), c->stream));
   if (col_end <= col_start) return DCU_OK;
   const int p = opt->precision;
-  const int max_ni = (p >= 0 && p < 5 && c->tune_set[p]) ? c->tune[p].group_max_ni : 0;
+  const bool tuned = p >= 0 && p < 5 && c->tune_set[p];
+  const int max_ni = tuned ? c->tune[p].group_max_ni : 0;
+  const int cta_max_area = tuned ? c->tune[p].cta_max_area : 0;
   // FP64 (the plain form): Householder on every column unless the normal
   // equations are asked for.  Mixed forms: the thread-per-column path first,
   // Householder for the columns it hands over, unless Householder is asked for.
   if (opt->precision == DCU_PREC_FP64)
     return build_typed<double>(c, n, ptr, idx, val, col_start, col_end, opt->schedule,
-                               opt->ls_method == DCU_LS_NORMAL_EQ, max_ni, mval, colres, info);
+                               opt->ls_method == DCU_LS_NORMAL_EQ, max_ni, cta_max_area, mval, colres, info);
   return build_typed<float>(c, n, ptr, idx, val, col_start, col_end, opt->schedule, opt->ls_method != DCU_LS_HOUSEHOLDER,
-                            max_ni, mval, colres, info);
+                            max_ni, cta_max_area, mval, colres, info);
 }
 
 int spai_pattern(Ctx* c, int n, const int* ptr, const int* idx, int col_start, int col_end, int* icount,

@@ -35,7 +35,7 @@ class Options(C.Structure):
 class BuildInfo(C.Structure):
     _fields_ = [("cols_total", C.c_int), ("cols_small", C.c_int), ("cols_large", C.c_int),
                 ("cols_singular", C.c_int), ("max_nj", C.c_int), ("max_ni", C.c_int), ("ms", C.c_float),
-                ("cols_staged", C.c_int)]
+                ("cols_staged", C.c_int), ("cols_hub", C.c_int)]
 
 
 class SolveInfo(C.Structure):
@@ -46,11 +46,12 @@ class SolveInfo(C.Structure):
 class Tuning(C.Structure):
     """dcu_tuning: launch configuration of one precision form and the autotuner's report."""
     _fields_ = [("k1_split", C.c_int), ("grid_p", C.c_int), ("grid_y", C.c_int), ("grid_py", C.c_int),
-                ("grid_sz", C.c_int), ("group_max_ni", C.c_int), ("iter_us_default", C.c_float),
+                ("grid_sz", C.c_int), ("group_max_ni", C.c_int), ("cta_max_area", C.c_int),
+                ("iter_us_default", C.c_float),
                 ("iter_us_tuned", C.c_float), ("build_ms_default", C.c_float), ("build_ms_tuned", C.c_float),
                 ("candidates", C.c_int)]
 
-    CONFIG = ("k1_split", "grid_p", "grid_y", "grid_py", "grid_sz", "group_max_ni")
+    CONFIG = ("k1_split", "grid_p", "grid_y", "grid_py", "grid_sz", "group_max_ni", "cta_max_area")
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}

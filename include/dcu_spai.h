@@ -106,6 +106,9 @@ typedef struct {
   float ms;               /* device time of the build (CUDA events)              */
   int cols_staged;        /* CTA-kernel columns whose J columns were brought into
                              shared memory by bulk (TMA) copies                    */
+  int cols_hub;           /* CTA-kernel columns whose dense block exceeded shared
+                             memory and was factored by the all-SM hub kernels
+                             (one launch per Householder step)                     */
 } dcu_build_info;
 
 typedef struct {
@@ -303,16 +306,23 @@ int dcu_sell_plan_stats(dcu_spai_ctx* ctx, long long* slots, long long* uniform_
  *   group_max_ni   SPAI build: largest |I_k| the warp-group (warp-per-small)
  *              kernel takes, 1..32 (0 = 32); larger columns go to the
  *              CTA-per-column kernel.  Changes M by rounding only.
+ *   cta_max_area   SPAI build: largest dense block |I_k| x (|J_k| + 1) one CTA
+ *              factors; a larger block is gathered into its own slab and
+ *              factored by the hub kernels, every SM on every such column.
+ *              0 = what fits the CTA's shared memory; -1 = no limit (every
+ *              block on one CTA, larger ones from a per-CTA global slab).
+ *              Changes M by rounding only.
  * The report fields are written by dcu_autotune_d and ignored on input. */
 typedef struct {
   int k1_split;
   int grid_p, grid_y, grid_py, grid_sz;
   int group_max_ni;
+  int cta_max_area;
   /* report */
   float iter_us_default;  /* solve ms / iterations with the default iteration configuration      */
   float iter_us_tuned;    /* the same with the chosen one                                         */
-  float build_ms_default; /* SPAI build with group_max_ni = 32                                   */
-  float build_ms_tuned;   /* SPAI build with the chosen group_max_ni                             */
+  float build_ms_default; /* SPAI build with the default build fields                            */
+  float build_ms_tuned;   /* SPAI build with the chosen ones                                      */
   int candidates;         /* launch configurations timed                                         */
 } dcu_tuning;
 
@@ -327,7 +337,8 @@ int dcu_get_tuning(dcu_spai_ctx* ctx, int precision, dcu_tuning* t);
 /* Time the candidate configurations of opt->precision on this matrix and
  * keep the fastest (as dcu_set_tuning would).  Steps: (1) two builds per
  * group_max_ni candidate (32, 24, 16; a candidate that would hand more than
- * 1/8 of the columns to the CTA kernel is not timed); (2) one solve of
+ * 1/8 of the columns to the CTA kernel is not timed), and with
+ * cta_max_area = -1 when the default build used the hub kernels; (2) one solve of
  * A x = b from x0 = 0 with the chosen build, then each kernel without a
  * reduction at grid selectors 0, -1 and half the resident blocks, `reps`
  * single launches each (<= 0: 10), every timed launch right after an untimed

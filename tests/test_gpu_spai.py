@@ -143,3 +143,34 @@ def test_bulk_copy_staging_matches_plain_loads(ctx):
     c1, p1, l1 = ctx.pattern_d(A.n, ptr, idx)
     c2, p2, l2 = ctx.pattern_d(A.n, ptr, idx_u)
     assert torch.equal(c1, c2) and torch.equal(l1, l2)
+
+
+@pytest.mark.parametrize("prec", [N.PREC_FP64, N.PREC_MIXED_BF16])
+def test_hub_kernels_match_one_cta_per_column(prec):
+    """Dense blocks larger than a CTA's shared memory (the circuit-like
+    matrix's hub columns) are factored by the all-SM hub kernels, one launch
+    per Householder step; with cta_max_area = -1 one CTA factors each from a
+    global slab, and with a limit in between both paths share the columns.
+    All agree with the oracle's Householder to the form's rounding, and the
+    hub path is deterministic."""
+    from dcu_b200.api import Context
+
+    A = W.circuit_like()
+    m_h, res_h, _, _ = oracle.spai(A, "householder")
+    with Context(0) as c:
+        m0, r0, i0 = c.build_h(A, precision=prec)
+        m0b, _, _ = c.build_h(A, precision=prec)
+        c.set_tuning(prec, cta_max_area=-1)
+        m1, r1, i1 = c.build_h(A, precision=prec)
+        c.set_tuning(prec, cta_max_area=200000)
+        m2, r2, i2 = c.build_h(A, precision=prec)
+    assert i0.cols_hub > 0 and i1.cols_hub == 0 and i2.cols_hub <= i0.cols_hub
+    assert i0.cols_large == i1.cols_large == i2.cols_large
+    assert np.array_equal(m0, m0b)
+    tol = RTOL_FP64 if prec == N.PREC_FP64 else RTOL_FP32 * 10
+    for m, r in ((m0, r0), (m1, r1), (m2, r2)):
+        for k in range(A.n):
+            a, b = m[A.ptr[k]:A.ptr[k + 1]], m_h[A.ptr[k]:A.ptr[k + 1]]
+            if len(b):
+                assert np.max(np.abs(a - b)) <= tol * np.max(np.abs(b)), (k, prec)
+        assert np.max(np.abs(r - res_h)) < (1e-10 if prec == N.PREC_FP64 else 1e-3)
