@@ -1132,64 +1132,80 @@ __global__ void __launch_bounds__(LG_BLOCK, 1) k_spai_large(LargeArgs a) {
 }
 
 // ---- hub kernels: columns whose dense block exceeds shared memory ---------
-// One launch per Householder step c, over every hub column at once: a warp
-// per trailing column j > c applies reflector c (the dot product and update
-// of the CTA kernel, lanes striding the rows), and the warp of column c + 1
-// then forms reflector c + 1 from its updated column.  Launch c = -1 forms
-// reflector 0.  Each hub's block streams through L2 on all SMs instead of
-// through one SM.  k_hub_solve then back-substitutes, one CTA per column.
-constexpr int HUB_BLOCK = 256;
+// One launch per Householder step c, over every hub column at once: a block
+// of HUB_THREADS per trailing column j > c applies reflector c (dot product
+// and update, threads striding the rows), and the block of column c + 1 then
+// forms reflector c + 1 from its updated column.  Launch c = -1 forms
+// reflector 0.  The hubs are sorted by |J| descending, so the hubs still
+// active at step c (|J| > c) are a prefix and block b finds its column by a
+// binary search on S(h) - c h, S = prefix sum of |J|.  Each hub's block
+// streams through L2 on all SMs instead of through one SM; the steps are
+// chained by programmatic dependent launch.  k_hub_solve then
+// back-substitutes, one CTA per column.
+constexpr int HUB_THREADS = 128;
+constexpr int HUB_WARPS = HUB_THREADS / 32;
 
 struct HubArgs {
-  const HubMeta* meta;
-  const int* wpre;  // wpre[h] = sum of (nj + 1) over hubs before h; warp w works in hub h when wpre[h] <= w
+  const HubMeta* meta;  // sorted by nj descending
+  const int* spre;      // spre[h] = sum of nj over hubs before h (nh + 1 entries)
   int nh;
-  int total_w;      // wpre[nh]
   void* pool;
 };
 
+// Sum of one double per thread of a HUB_THREADS block, in a fixed order.
+__device__ __forceinline__ double hub_sum(double v, double* red) {
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+#pragma unroll
+  for (int w = 0; w < HUB_WARPS; ++w) t += red[w];
+  return t;
+}
+
+// Step c: `active` = hubs with nj > c (a prefix of the sorted list); the grid
+// has sum over them of (nj - c) blocks.
 template <typename T>
-__global__ void __launch_bounds__(HUB_BLOCK) k_hub_step(HubArgs h, int c) {
-  const int gw = (int)(((long long)blockIdx.x * HUB_BLOCK + threadIdx.x) >> 5);
-  const int lane = threadIdx.x & 31;
-  if (gw >= h.total_w) return;
-  int lo = 0, hi = h.nh - 1;
+__global__ void __launch_bounds__(HUB_THREADS) k_hub_step(HubArgs h, int c, int active) {
+  __shared__ double red[HUB_WARPS];
+  const int tid = threadIdx.x;
+  const int b = blockIdx.x;
+  // largest hub index g < active with spre[g] - c g <= b
+  int lo = 0, hi = active - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
-    if (h.wpre[mid] <= gw) lo = mid;
+    if ((long long)h.spre[mid] - (long long)c * mid <= b) lo = mid;
     else hi = mid - 1;
   }
   const HubMeta hm = h.meta[lo];
-  const int W = hm.nj + 1;
-  const int j = c + 1 + (gw - h.wpre[lo]);
-  if (j >= W) return;
-  const int m = hm.m;
+  const int j = c + 1 + (b - (int)((long long)h.spre[lo] - (long long)c * lo));
+  const int m = hm.m, W = hm.nj + 1;
   const int steps = min(hm.nj, m);
   T* Ad = reinterpret_cast<T*>(h.pool) + hm.off;
   T* rd = Ad + (long long)m * W;
   T* bt = rd + W;
   T* aj = Ad + (long long)j * m;
+  cudaGridDependencySynchronize();  // step c - 1 has finished: reflector c and column j are current
   if (c >= 0 && c < steps) {
     const T beta = bt[c];
     if (beta != T(0)) {
       const T* vc = Ad + (long long)c * m;
-      T w = T(0);
-      for (int i = c + lane; i < m; i += 32) w += vc[i] * aj[i];
-#pragma unroll
-      for (int d = 16; d > 0; d >>= 1) w += __shfl_xor_sync(0xffffffffu, w, d);
-      w *= beta;
-      for (int i = c + lane; i < m; i += 32) aj[i] -= w * vc[i];
+      double part = 0.0;
+      for (int i = c + tid; i < m; i += HUB_THREADS) part += (double)(vc[i] * aj[i]);
+      const T w = (T)hub_sum(part, red) * beta;
+      for (int i = c + tid; i < m; i += HUB_THREADS) aj[i] -= w * vc[i];
     }
   }
   if (j == c + 1 && j < steps) {
+    __syncthreads();  // the update above wrote these rows from other threads
     double part = 0.0;
-    for (int i = j + lane; i < m; i += 32) part += (double)aj[i] * (double)aj[i];
-#pragma unroll
-    for (int d = 16; d > 0; d >>= 1) part += __shfl_xor_sync(0xffffffffu, part, d);
-    __syncwarp();  // aj[j] was updated by another lane
-    if (lane == 0) {
+    for (int i = j + tid; i < m; i += HUB_THREADS) part += (double)aj[i] * (double)aj[i];
+    const double nrm2 = hub_sum(part, red);
+    if (tid == 0) {
       const T x0 = aj[j];
-      const T nrm = (T)sqrt(part);
+      const T nrm = (T)sqrt(nrm2);
       T alpha = T(0), beta = T(0);
       if (nrm > T(0)) {
         alpha = (x0 > T(0)) ? -nrm : nrm;
@@ -1205,6 +1221,7 @@ __global__ void __launch_bounds__(HUB_BLOCK) k_hub_step(HubArgs h, int c) {
 template <typename T>
 __global__ void __launch_bounds__(LG_BLOCK) k_hub_solve(HubArgs h, LargeArgs a) {
   __shared__ T ys[LG_NJ_MAX];
+  __shared__ T xs[LG_NJ_MAX];
   __shared__ double red[LG_WARPS];
   const HubMeta hm = h.meta[blockIdx.x];
   const int tid = threadIdx.x;
@@ -1217,20 +1234,22 @@ __global__ void __launch_bounds__(LG_BLOCK) k_hub_solve(HubArgs h, LargeArgs a) 
   for (int i = nj + tid; i < m; i += LG_BLOCK) part += (double)y[i] * (double)y[i];
   const double res2 = block_sum(part, red);
   __syncthreads();
+  // One barrier per row: every thread forms x_i = ys_i / R_ii itself (ys_i
+  // is final once row i + 1 is done), thread 0 records it, and the rows above
+  // are updated; ys_i itself is never written again.
   bool sing = m < nj;
   for (int i = nj - 1; i >= 0; --i) {
+    const T rii = (i < m) ? rd[i] : T(0);
+    const T xi = ys[i] / rii;
     if (tid == 0) {
-      const T rii = (i < m) ? rd[i] : T(0);
       if (!(rii != T(0)) || !isfinite((double)rii)) sing = true;
-      ys[i] = ys[i] / rii;
+      xs[i] = xi;
     }
-    __syncthreads();
-    const T xi = ys[i];
     for (int t = tid; t < min(i, m); t += LG_BLOCK) ys[t] -= Ad[(long long)i * m + t] * xi;
     __syncthreads();
   }
   const int cs = a.ptr[hm.k];
-  for (int t = tid; t < nj; t += LG_BLOCK) a.mval[cs + t] = (double)ys[t];
+  for (int t = tid; t < nj; t += LG_BLOCK) a.mval[cs + t] = (double)xs[t];
   if (tid == 0) {
     if (a.colres) a.colres[hm.k - a.col_start] = sqrt(res2);
     if (sing) atomicAdd(&a.stats[ST_SINGULAR], 1);
@@ -1320,8 +1339,9 @@ int run_large(Ctx* c, LargeArgs& a, int nbig, int cta_max_area = 0) {
   k_spai_large<T, MODE><<<grid, LG_BLOCK, smem, c->stream>>>(a);
   DCU_LAUNCHED(c, "k_spai_large");
   if (!a.hub_pool) return DCU_OK;
-  // hub columns: read their descriptors, map warps to (column, trailing
-  // column), one step launch per Householder step, then the solves
+  // hub columns: read their descriptors, sort them by |J| descending, one
+  // step launch per Householder step over the hubs still active, then the
+  // solves
   int* st = bp<int>(c, B_STATS);
   DCU_CUDA(c, cudaMemcpyAsync(c->pinned, st + ST_HUB_COUNT, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   DCU_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -1331,20 +1351,34 @@ int run_large(Ctx* c, LargeArgs& a, int nbig, int cta_max_area = 0) {
   DCU_CUDA(c, cudaMemcpyAsync(hm.data(), a.hub_meta, sizeof(HubMeta) * (size_t)nh, cudaMemcpyDeviceToHost,
                               c->stream));
   DCU_CUDA(c, cudaStreamSynchronize(c->stream));
-  std::vector<int> wpre((size_t)nh + 1, 0);
+  std::stable_sort(hm.begin(), hm.end(), [](const HubMeta& x, const HubMeta& y) { return x.nj > y.nj; });
+  std::vector<int> spre((size_t)nh + 1, 0);
   int steps = 0;
-  for (int h = 0; h < nh; ++h) {
-    wpre[h + 1] = wpre[h] + hm[h].nj + 1;
-    steps = std::max(steps, std::min(hm[h].nj, hm[h].m));
+  for (int g = 0; g < nh; ++g) {
+    spre[g + 1] = spre[g] + hm[g].nj;
+    steps = std::max(steps, std::min(hm[g].nj, hm[g].m));
   }
-  DCU_TRY(ensure(c, B_HUBWPRE, sizeof(int) * wpre.size()));
-  DCU_CUDA(c, cudaMemcpyAsync(c->buf[B_HUBWPRE].p, wpre.data(), sizeof(int) * wpre.size(), cudaMemcpyHostToDevice,
+  DCU_TRY(ensure(c, B_HUBWPRE, sizeof(int) * spre.size()));
+  DCU_CUDA(c, cudaMemcpyAsync(a.hub_meta, hm.data(), sizeof(HubMeta) * (size_t)nh, cudaMemcpyHostToDevice,
                               c->stream));
-  HubArgs h{a.hub_meta, bp<int>(c, B_HUBWPRE), nh, wpre[nh], a.hub_pool};
-  const int blocks = (int)(((long long)wpre[nh] * 32 + HUB_BLOCK - 1) / HUB_BLOCK);
+  DCU_CUDA(c, cudaMemcpyAsync(c->buf[B_HUBWPRE].p, spre.data(), sizeof(int) * spre.size(), cudaMemcpyHostToDevice,
+                              c->stream));
+  HubArgs h{a.hub_meta, bp<int>(c, B_HUBWPRE), nh, a.hub_pool};
+  int active = nh;
   for (int cst = -1; cst < steps; ++cst) {
-    k_hub_step<T><<<blocks, HUB_BLOCK, 0, c->stream>>>(h, cst);
-    DCU_LAUNCHED(c, "k_hub_step");
+    while (active > 0 && hm[active - 1].nj <= cst) --active;  // hubs with nj > cst
+    const long long blocks = (long long)spre[active] - (long long)cst * active;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)blocks);
+    cfg.blockDim = dim3(HUB_THREADS);
+    cfg.stream = c->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = cst >= 0 ? 1 : 0;  // the first step follows copies, not a step
+    DCU_CUDA(c, cudaLaunchKernelEx(&cfg, k_hub_step<T>, h, cst, active));
+    c->launches++;
   }
   k_hub_solve<T><<<nh, LG_BLOCK, 0, c->stream>>>(h, a);
   DCU_LAUNCHED(c, "k_hub_solve");
