@@ -1236,16 +1236,36 @@ __global__ void __launch_bounds__(LG_BLOCK) k_hub_solve(HubArgs h, LargeArgs a) 
   __syncthreads();
   // One barrier per row: every thread forms x_i = ys_i / R_ii itself (ys_i
   // is final once row i + 1 is done), thread 0 records it, and the rows above
-  // are updated; ys_i itself is never written again.
+  // are updated; ys_i itself is never written again.  R_ii and this thread's
+  // entries of column i are loaded during row i + 1, so no global load sits
+  // on the per-row chain.
+  constexpr int PT = LG_NJ_MAX / LG_BLOCK;  // rows of R per thread
+  auto load_col = [&](int i, T (&v)[PT], T& r) {
+    r = (i < m) ? rd[i] : T(0);
+#pragma unroll
+    for (int q = 0; q < PT; ++q) {
+      const int t = tid + q * LG_BLOCK;
+      v[q] = (t < min(i, m)) ? Ad[(long long)i * m + t] : T(0);
+    }
+  };
   bool sing = m < nj;
+  T cur[PT], nxt[PT], rii = T(0), rnx = T(0);
+  if (nj > 0) load_col(nj - 1, cur, rii);
   for (int i = nj - 1; i >= 0; --i) {
-    const T rii = (i < m) ? rd[i] : T(0);
     const T xi = ys[i] / rii;
     if (tid == 0) {
       if (!(rii != T(0)) || !isfinite((double)rii)) sing = true;
       xs[i] = xi;
     }
-    for (int t = tid; t < min(i, m); t += LG_BLOCK) ys[t] -= Ad[(long long)i * m + t] * xi;
+    if (i > 0) load_col(i - 1, nxt, rnx);
+#pragma unroll
+    for (int q = 0; q < PT; ++q) {
+      const int t = tid + q * LG_BLOCK;
+      if (t < min(i, m)) ys[t] -= cur[q] * xi;
+    }
+#pragma unroll
+    for (int q = 0; q < PT; ++q) cur[q] = nxt[q];
+    rii = rnx;
     __syncthreads();
   }
   const int cs = a.ptr[hm.k];

@@ -174,3 +174,35 @@ def test_hub_kernels_match_one_cta_per_column(prec):
             if len(b):
                 assert np.max(np.abs(a - b)) <= tol * np.max(np.abs(b)), (k, prec)
         assert np.max(np.abs(r - res_h)) < (1e-10 if prec == N.PREC_FP64 else 1e-3)
+
+
+def rank_deficient_hub(n=400, seed=5):
+    """Column 0 has rows 1..300 (|J| = 300), and each of those columns has
+    three rows among 0..49, so |I_0| <= 50 < |J_0|: a rank-deficient least-
+    squares problem whose block (<= 50 x 301) exceeds shared memory."""
+    rng = np.random.default_rng(seed)
+    cols = [(np.arange(1, 301), rng.standard_normal(300))]
+    for _ in range(1, 301):
+        cols.append((np.sort(rng.choice(50, 3, replace=False)), rng.standard_normal(3)))
+    for j in range(301, n):
+        cols.append((np.array([j]), np.array([2.0])))
+    ptr = np.zeros(n + 1, np.int32)
+    for j, (r, _) in enumerate(cols):
+        ptr[j + 1] = ptr[j] + len(r)
+    idx = np.concatenate([c[0] for c in cols]).astype(np.int32)
+    val = np.concatenate([c[1] for c in cols])
+    return W.CSC(n, ptr, idx, val)
+
+
+def test_hub_column_with_fewer_rows_than_columns(ctx):
+    """The hub path on |I| < |J|: the column is reported singular (as by the
+    oracle's Householder), R's missing rows are never read, and every other
+    column matches the oracle."""
+    A = rank_deficient_hub()
+    m_h, res_h, _, sing = oracle.spai(A, "householder")
+    m, res, info = ctx.build_h(A)
+    assert info.cols_hub >= 1 and sing == 1 and info.cols_singular == sing
+    assert not np.all(np.isfinite(m[A.ptr[0]:A.ptr[1]]))
+    for k in range(1, A.n):
+        a, b = m[A.ptr[k]:A.ptr[k + 1]], m_h[A.ptr[k]:A.ptr[k + 1]]
+        assert np.max(np.abs(a - b)) <= RTOL_FP64 * max(1.0, np.max(np.abs(b))), k
