@@ -330,8 +330,12 @@ __device__ __forceinline__ int group_column(const SmallArgs& a, WarpSmem<T>& ws,
   return m;
 }
 
+// Held to 80 registers (12 blocks, 24 warps per SM): the Householder steps are
+// latency-bound, and at the unbounded 128 registers only 8 blocks fit (FP64
+// build at 128^3: 7.06 -> 5.92 ms, M bit-identical; at 64 registers it spills
+// and takes 6.3 ms).
 template <typename T, int MODE>
-__global__ void __launch_bounds__(SG_BLOCK) k_spai_small(SmallArgs a) {
+__global__ void __launch_bounds__(SG_BLOCK, 12) k_spai_small(SmallArgs a) {
   __shared__ WarpSmem<T> smem[SG_WARPS];
   const int lane = threadIdx.x & (GL - 1);
   const int g = (threadIdx.x / GL) & (SG_GPW - 1);
