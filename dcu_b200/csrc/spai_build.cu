@@ -1349,12 +1349,18 @@ int run_large(Ctx* c, LargeArgs& a, int nbig, int cta_max_area = 0) {
   a.hub_min_area = a.smem_area > cta_max_area ? a.smem_area : cta_max_area;
   if (MODE == MODE_BUILD && a.area_per_block > a.hub_min_area && cta_max_area >= 0) {
     a.hub_cap = a.area_sum < kHubPoolMax ? a.area_sum : kHubPoolMax;
-    DCU_TRY(ensure(c, B_HUBPOOL, sizeof(T) * (size_t)a.hub_cap));
-    DCU_TRY(ensure(c, B_HUBMETA, sizeof(HubMeta) * (size_t)nbig));
-    a.hub_pool = c->buf[B_HUBPOOL].p;
-    a.hub_meta = bp<HubMeta>(c, B_HUBMETA);
-    // the pool holds every block above shared memory: no per-CTA slabs
-    if (a.hub_cap == a.area_sum && a.hub_min_area == a.smem_area) a.area_per_block = 0;
+    // without room for the pool every block stays on one CTA (per-CTA slabs)
+    const std::string err = c->err;
+    if (ensure(c, B_HUBPOOL, sizeof(T) * (size_t)a.hub_cap) == DCU_OK &&
+        ensure(c, B_HUBMETA, sizeof(HubMeta) * (size_t)nbig) == DCU_OK) {
+      a.hub_pool = c->buf[B_HUBPOOL].p;
+      a.hub_meta = bp<HubMeta>(c, B_HUBMETA);
+      // the pool holds every block above shared memory: no per-CTA slabs
+      if (a.hub_cap == a.area_sum && a.hub_min_area == a.smem_area) a.area_per_block = 0;
+    } else {
+      c->err = err;
+      a.hub_cap = 0;
+    }
   }
   DCU_TRY(ensure(c, B_SLAB_BITS, sizeof(unsigned) * 2 * (size_t)a.words_per_block * grid));
   a.gbits = bp<unsigned>(c, B_SLAB_BITS);
