@@ -156,11 +156,12 @@ class Context:
         self._check(self._L.dcu_profile_iteration_kernels(self.h, reps, ms, 16, C.byref(cnt)))
         return [float(ms[i]) for i in range(cnt.value)]
 
-    def sell_plan_stats(self):
-        """(slots, uniform_slots) of the last SELL layout built on this context."""
-        s, u = C.c_longlong(), C.c_longlong()
-        self._check(self._L.dcu_sell_plan_stats(self.h, C.byref(s), C.byref(u)))
-        return s.value, u.value
+    def sell_plan_stats(self, wide: bool = False):
+        """(slots, uniform_slots) of the last SELL layout built on this context; with wide=True also the
+        number of full slices wider than 64 slots (summed by the warp-cooperative pre-pass)."""
+        s, u, w = C.c_longlong(), C.c_longlong(), C.c_longlong()
+        self._check(self._L.dcu_sell_plan_stats(self.h, C.byref(s), C.byref(u), C.byref(w)))
+        return (s.value, u.value, w.value) if wide else (s.value, u.value)
 
     def autotune_d(self, n, nnz, ptr_d, idx_d, val_d, b_d, reps: int = 10, **opt) -> "N.Tuning":
         """Time the launch configurations of opt's precision form on this matrix and keep the fastest

@@ -134,7 +134,7 @@ __device__ __forceinline__ void sell_row_v(const long long* __restrict__ off, co
         for (int e = 0; e < V; ++e) acc[e] += av[t] * xv[e];
       }
   };
-  if (__ldg(su + sl)) {
+  if (__ldg(su + sl) & 1) {
     const int* __restrict__ kp = kd + (o0 >> 5);
     for (int k0 = 0; k0 < w; k0 += 8) {
       double av[8];

@@ -66,17 +66,20 @@ __device__ __forceinline__ double ldv(const T* p) { return (double)__ldg(p); }
 // keeps up to 16 independent loads in flight.  A slice whose every k has one
 // column offset for all its rows (su[s]; SellPlan::kd) reads no index at all:
 // the column is the row plus the slice's offset, one broadcast load per k
-// from a table 1/32 the size of the index array.
+// from a table 1/32 the size of the index array.  The rows of a slice wider
+// than kWideSlice were summed by the wide pre-pass (k_bi_wide) into wv.
 template <typename MT, typename IT, typename F>
 __device__ __forceinline__ double sell_row(const long long* __restrict__ off, const int* __restrict__ kd,
-                                           const int* __restrict__ su, const MT* __restrict__ val,
-                                           const IT* __restrict__ ix, int r, F xf) {
+                                           const int* __restrict__ su, const double* __restrict__ wv,
+                                           const MT* __restrict__ val, const IT* __restrict__ ix, int r, F xf) {
   const int s = r >> 5;
+  const int f = __ldg(su + s);
+  if (f & 4) return __ldg(wv + ((long long)(f >> 3) << 5) + (r & 31));
   const long long o0 = __ldg(off + s), o1 = __ldg(off + s + 1);
   const long long base = o0 + (r & 31);
   const int w = (int)((o1 - o0) >> 5);
   double acc = 0.0;
-  if (__ldg(su + s)) {
+  if (f & 1) {
     const int* __restrict__ kp = kd + (o0 >> 5);
     for (int k0 = 0; k0 < w; k0 += 8) {
       double av[8];
@@ -189,6 +192,10 @@ struct BiArgs {
   double* az;
   double* part;
   Scal* S;
+  const int* rptr;       // CSR row pointers (row lengths of the wide slices)
+  const int* wide_list;  // slices wider than kWideSlice (SellPlan::wide)
+  double* wide_val;      // their row values for the next SpMV, 32 per listed slice
+  int nwide;
 };
 
 // Kernels K1..K5 are launched with programmatic dependent launch: their blocks
@@ -200,6 +207,118 @@ __device__ __forceinline__ bool finished(const Scal* S) {
 
 __device__ __forceinline__ bool bad(double v) { return !isfinite(v); }
 
+// ---- wide pre-pass ---------------------------------------------------------
+// A full slice wider than kWideSlice holds a long row; in sell_row its warp
+// would walk every slot of the slice, with one gather latency per 8 slots.
+// Here a warp takes one such slice: each lane sums its own row up to its own
+// length (rptr), 8 slots at a time as in sell_row; then the rows longer than
+// kWideSlice are summed one at a time by the whole warp, each lane loading one
+// entry in 32 and its gather (the next 32 prefetched), and one chain of
+// multiply-adds consuming them in k order through shuffles.  Every row's sum
+// is formed in sell_row's order with its operations, stopping at the row's
+// length instead of running over the zero padding, so the iterates do not
+// change.  Launched just before the kernel whose SpMV it serves.
+enum { WIDE_AX = 0, WIDE_PY, WIDE_Y, WIDE_AY, WIDE_SZ, WIDE_AZ };
+
+template <typename MT, typename IT, typename F>
+__device__ __forceinline__ double wide_row(long long o0, const int* __restrict__ rptr, const MT* __restrict__ val,
+                                           const IT* __restrict__ ix, int r, F xf) {
+  const int lane = r & 31;
+  const int len = __ldg(rptr + r + 1) - __ldg(rptr + r);
+  const long long base = o0 + lane;
+  double acc = 0.0;
+  if (len <= kWideSlice) {
+    for (int k0 = 0; k0 < len; k0 += 8) {
+      double av[8];
+      int cv[8];
+#pragma unroll
+      for (int t = 0; t < 8; ++t) {
+        if (k0 + t < len) {
+          const long long q = base + 32ll * (k0 + t);
+          av[t] = ldm(val + q);
+          cv[t] = ldcol(ix, q, r);
+        } else {
+          av[t] = 0.0;
+          cv[t] = r;
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < 8; ++t)
+        if (k0 + t < len) acc += av[t] * xf(cv[t]);
+    }
+  }
+  unsigned longs = __ballot_sync(0xffffffffu, len > kWideSlice);
+  while (longs) {
+    const int j = __ffs(longs) - 1;
+    longs &= longs - 1;
+    const int lj = __shfl_sync(0xffffffffu, len, j);
+    const int rj = (r & ~31) + j;
+    const long long bj = o0 + j;
+    auto load = [&](int k, double& av, double& xv) {
+      if (k < lj) {
+        const long long q = bj + 32ll * k;
+        av = ldm(val + q);
+        xv = xf(ldcol(ix, q, rj));
+      } else {
+        av = 0.0;
+        xv = 0.0;
+      }
+    };
+    double chain = 0.0, av0, xv0;
+    load(lane, av0, xv0);
+    for (int c0 = 0; c0 < lj; c0 += 32) {
+      double av1, xv1;
+      load(c0 + 32 + lane, av1, xv1);
+      const int cnt = min(32, lj - c0);
+      for (int t = 0; t < cnt; ++t) {
+        const double at = __shfl_sync(0xffffffffu, av0, t);
+        const double xt = __shfl_sync(0xffffffffu, xv0, t);
+        chain += at * xt;
+      }
+      av0 = av1;
+      xv0 = xv1;
+    }
+    if (lane == j) acc = chain;
+  }
+  return acc;
+}
+
+template <typename MT, typename IT, typename VT, int WHICH>
+__global__ void __launch_bounds__(BI_BLOCK) k_bi_wide(BiArgs<MT, IT, VT> a) {
+  if (WHICH != WIDE_AX && finished(a.S)) return;  // WIDE_AX serves k_bi_init / k_bi_true (plain launches)
+  const int wv = (int)(((long long)blockIdx.x * BI_BLOCK + threadIdx.x) >> 5);
+  if (wv >= a.nwide) return;  // whole warps
+  const int s = a.wide_list[wv];
+  const int r = (s << 5) + (threadIdx.x & 31);
+  const long long o0 = a.off[s];
+  double v;
+  if constexpr (WHICH == WIDE_AX) {
+    v = wide_row(o0, a.rptr, a.aval, a.ix, r, [&](int c) { return ldv(a.x + c); });
+  } else if constexpr (WHICH == WIDE_PY) {
+    const double beta = a.S->beta, omega = a.S->omega;
+    const VT* __restrict__ pold = a.S->pidx ? a.p1 : a.p0;
+    const double* __restrict__ rr = a.r;
+    const double* __restrict__ ay = a.ay;
+    v = wide_row(o0, a.rptr, a.mval, a.ix, r,
+                 [&](int c) { return ldv(rr + c) + beta * (ldv(pold + c) - omega * ldv(ay + c)); });
+  } else if constexpr (WHICH == WIDE_Y) {
+    const VT* __restrict__ p = a.p0;
+    v = wide_row(o0, a.rptr, a.mval, a.ix, r, [&](int c) { return ldv(p + c); });
+  } else if constexpr (WHICH == WIDE_AY) {
+    const VT* __restrict__ y = a.y;
+    v = wide_row(o0, a.rptr, a.aval, a.ix, r, [&](int c) { return ldv(y + c); });
+  } else if constexpr (WHICH == WIDE_SZ) {
+    const double nalpha = -1.0 * a.S->alpha;
+    const double* __restrict__ rr = a.r;
+    const double* __restrict__ ay = a.ay;
+    v = wide_row(o0, a.rptr, a.mval, a.ix, r, [&](int c) { return ldv(rr + c) + nalpha * ldv(ay + c); });
+  } else {
+    const VT* __restrict__ z = a.z;
+    v = wide_row(o0, a.rptr, a.aval, a.ix, r, [&](int c) { return ldv(z + c); });
+  }
+  a.wide_val[((long long)wv << 5) + (threadIdx.x & 31)] = v;
+}
+
 // K0: r = b - A x, r* = r, p = ay = 0, rho = (r*, r), ||r||, ||b||
 template <typename MT, typename IT, typename VT>
 __global__ void __launch_bounds__(BI_BLOCK) k_bi_init(BiArgs<MT, IT, VT> a, double tol, int tol_mode, int maxiter,
@@ -207,7 +326,7 @@ __global__ void __launch_bounds__(BI_BLOCK) k_bi_init(BiArgs<MT, IT, VT> a, doub
   double v[3] = {0.0, 0.0, 0.0};
   const int stride = gridDim.x * BI_BLOCK;
   for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) {
-    const double ax = sell_row(a.off, a.kd, a.su, a.aval, a.ix, r, [&](int c) { return ldv(a.x + c); });
+    const double ax = sell_row(a.off, a.kd, a.su, a.wide_val, a.aval, a.ix, r, [&](int c) { return ldv(a.x + c); });
     const double br = a.b[r];
     const double rr = br + (-1.0) * ax;
     a.r[r] = rr;
@@ -262,7 +381,7 @@ __global__ void __launch_bounds__(BI_BLOCK) k_bi_py(BiArgs<MT, IT, VT> a) {
   auto pf = [&](int c) { return ldv(rr + c) + beta * (ldv(pold + c) - omega * ldv(ay + c)); };
   const int stride = gridDim.x * BI_BLOCK;
   for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) {
-    const double yv = sell_row(a.off, a.kd, a.su, a.mval, a.ix, r, pf);
+    const double yv = sell_row(a.off, a.kd, a.su, a.wide_val, a.mval, a.ix, r, pf);
     pnew[r] = (VT)pf(r);
     a.y[r] = (VT)yv;
   }
@@ -320,18 +439,22 @@ __global__ void __launch_bounds__(BI_BLOCK, 8) k_bi_y(BiArgs<MT, IT, VT> a) {
   const VT* __restrict__ p = a.p0;
   const int stride = gridDim.x * BI_BLOCK;
   for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride)
-    a.y[r] = (VT)sell_row(a.off, a.kd, a.su, a.mval, a.ix, r, [&](int c) { return ldv(p + c); });
+    a.y[r] = (VT)sell_row(a.off, a.kd, a.su, a.wide_val, a.mval, a.ix, r, [&](int c) { return ldv(p + c); });
 }
 
 // K2: ay = A y; alpha = rho / (r*, ay)
+// 32 registers (8 blocks per SM) with 16-bit columns and a narrow M; with
+// int32 columns or an FP64 M up to 48 without spilling (5 blocks).  (An
+// explicit minimum of one block lets the compiler take 64 for the former.)
 template <typename MT, typename IT, typename VT>
-__global__ void __launch_bounds__(BI_BLOCK) k_bi_ay(BiArgs<MT, IT, VT> a) {
+__global__ void __launch_bounds__(BI_BLOCK, (std::is_same<MT, double>::value || std::is_same<IT, int>::value) ? 5 : 8)
+    k_bi_ay(BiArgs<MT, IT, VT> a) {
   if (finished(a.S)) return;
   double v[1] = {0.0};
   const VT* __restrict__ y = a.y;
   const int stride = gridDim.x * BI_BLOCK;
   for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) {
-    const double ayv = sell_row(a.off, a.kd, a.su, a.aval, a.ix, r, [&](int c) { return ldv(y + c); });
+    const double ayv = sell_row(a.off, a.kd, a.su, a.wide_val, a.aval, a.ix, r, [&](int c) { return ldv(y + c); });
     a.ay[r] = ayv;
     v[0] += (double)a.rs[r] * ayv;
   }
@@ -357,7 +480,7 @@ __global__ void __launch_bounds__(BI_BLOCK) k_bi_sz(BiArgs<MT, IT, VT> a) {
   auto sf = [&](int c) { return ldv(rr + c) + nalpha * ldv(ay + c); };
   const int stride = gridDim.x * BI_BLOCK;
   for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) {
-    const double zv = sell_row(a.off, a.kd, a.su, a.mval, a.ix, r, sf);
+    const double zv = sell_row(a.off, a.kd, a.su, a.wide_val, a.mval, a.ix, r, sf);
     a.s[r] = rr[r] + nalpha * ay[r];
     a.z[r] = (VT)zv;
   }
@@ -371,7 +494,7 @@ __global__ void __launch_bounds__(BI_BLOCK) k_bi_az(BiArgs<MT, IT, VT> a) {
   const VT* __restrict__ z = a.z;
   const int stride = gridDim.x * BI_BLOCK;
   for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) {
-    const double azv = sell_row(a.off, a.kd, a.su, a.aval, a.ix, r, [&](int c) { return ldv(z + c); });
+    const double azv = sell_row(a.off, a.kd, a.su, a.wide_val, a.aval, a.ix, r, [&](int c) { return ldv(z + c); });
     a.az[r] = azv;
     v[0] += azv * a.s[r];
     v[1] += azv * azv;
@@ -466,7 +589,7 @@ __global__ void __launch_bounds__(BI_BLOCK) k_bi_true(BiArgs<MT, IT, VT> a, int 
   double v[2] = {0.0, 0.0};
   const int stride = gridDim.x * BI_BLOCK;
   for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) {
-    const double ax = sell_row(a.off, a.kd, a.su, a.aval, a.ix, r, [&](int c) { return ldv(a.x + c); });
+    const double ax = sell_row(a.off, a.kd, a.su, a.wide_val, a.aval, a.ix, r, [&](int c) { return ldv(a.x + c); });
     const double rt = a.b[r] - ax;
     if (replace) a.r[r] = rt;
     v[0] += (double)a.rs[r] * rt;
@@ -600,11 +723,25 @@ int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval,
   a.z = (VT*)(base + 4 * nd + 4 * nv);
   a.part = bp<double>(c, B_PART);
   a.S = bp<Scal>(c, B_SCAL);
+  // slices wider than kWideSlice: their rows come from the wide pre-pass
+  a.rptr = plan.rptr;
+  a.wide_list = plan.wide;
+  a.nwide = plan.nwide;
+  if (plan.nwide > 0) {
+    DCU_TRY(ensure(c, B_WIDEVAL, sizeof(double) * 32 * (size_t)plan.nwide));
+    a.wide_val = bp<double>(c, B_WIDEVAL);
+  }
+  const int g_wide = (int)(((long long)plan.nwide * 32 + BI_BLOCK - 1) / BI_BLOCK);
+  const bool wide = plan.nwide > 0;
   if (reinterpret_cast<uintptr_t>(x) % 16 != 0)
     return fail(c, DCU_ERR_ARG, "x must be 16-byte aligned (cudaMalloc pointers are)");
   DCU_CUDA(c, cudaMemsetAsync(a.S, 0, sizeof(Scal), c->stream));
   int maxiter = opt->maxiter > 0 ? opt->maxiter : n;  // bicgstab_solver.h:134
   DCU_CUDA(c, cudaEventRecord(c->ev[0], c->stream));
+  if (wide) {
+    k_bi_wide<MT, IT, VT, WIDE_AX><<<g_wide, BI_BLOCK, 0, c->stream>>>(a);
+    DCU_LAUNCHED(c, "k_bi_wide");
+  }
   k_bi_init<MT, IT, VT><<<g_init, BI_BLOCK, 0, c->stream>>>(a, opt->tol, opt->tol_mode, maxiter, opt->verify);
   DCU_LAUNCHED(c, "k_bi_init");
 
@@ -624,15 +761,24 @@ int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval,
     cudaGraph_t g = nullptr;
     DCU_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     cudaError_t le = cudaSuccess;
+    // a wide pre-pass node ahead of each SpMV kernel when the layout has wide slices
+    auto pre = [&](auto kernel) {
+      if (wide && le == cudaSuccess) le = launch_pdl(kernel, g_wide, c->stream, a);
+    };
     for (int i = 0; i < CHUNK_ITERS && le == cudaSuccess; ++i) {
       if (split) {
         le = launch_pdl(k_bi_p<MT, IT, VT>, g_p, c->stream, a);
+        pre(k_bi_wide<MT, IT, VT, WIDE_Y>);
         if (le == cudaSuccess) le = launch_pdl(k_bi_y<MT, IT, VT>, g_y, c->stream, a);
       } else {
-        le = launch_pdl(k_bi_py<MT, IT, VT>, g_py, c->stream, a);
+        pre(k_bi_wide<MT, IT, VT, WIDE_PY>);
+        if (le == cudaSuccess) le = launch_pdl(k_bi_py<MT, IT, VT>, g_py, c->stream, a);
       }
+      pre(k_bi_wide<MT, IT, VT, WIDE_AY>);
       if (le == cudaSuccess) le = launch_pdl(k_bi_ay<MT, IT, VT>, g_ay, c->stream, a);
+      pre(k_bi_wide<MT, IT, VT, WIDE_SZ>);
       if (le == cudaSuccess) le = launch_pdl(k_bi_sz<MT, IT, VT>, g_sz, c->stream, a);
+      pre(k_bi_wide<MT, IT, VT, WIDE_AZ>);
       if (le == cudaSuccess) le = launch_pdl(k_bi_az<MT, IT, VT>, g_az, c->stream, a);
       if (le == cudaSuccess) le = launch_pdl(k_bi_xr<MT, IT, VT>, g_xr, c->stream, a);
     }
@@ -644,7 +790,7 @@ int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval,
     if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture", __FILE__, __LINE__);
     GraphSlot ne;
     ne.key = key;
-    ne.nodes = (split ? 6 : 5) * CHUNK_ITERS;
+    ne.nodes = ((split ? 6 : 5) + (wide ? 4 : 0)) * CHUNK_ITERS;
     e = cudaGraphInstantiate(&ne.exec, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return cuda_fail(c, e, "cudaGraphInstantiate", __FILE__, __LINE__);
@@ -709,6 +855,10 @@ int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval,
     DCU_CUDA(c, cudaStreamSynchronize(c->stream));
     hs = *pin;
     if (hs.verify_pending) {
+      if (wide) {
+        k_bi_wide<MT, IT, VT, WIDE_AX><<<g_wide, BI_BLOCK, 0, c->stream>>>(a);
+        DCU_LAUNCHED(c, "k_bi_wide");
+      }
       k_bi_true<MT, IT, VT><<<g_tr, BI_BLOCK, 0, c->stream>>>(a, 1);
       DCU_LAUNCHED(c, "k_bi_true");
       DCU_CUDA(c, cudaMemcpyAsync(pin, a.S, sizeof(Scal), cudaMemcpyDeviceToHost, c->stream));
@@ -719,6 +869,10 @@ int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval,
     break;
   }
   if (hs.true_res < 0.0) {
+    if (wide) {
+      k_bi_wide<MT, IT, VT, WIDE_AX><<<g_wide, BI_BLOCK, 0, c->stream>>>(a);
+      DCU_LAUNCHED(c, "k_bi_wide");
+    }
     k_bi_true<MT, IT, VT><<<g_tr, BI_BLOCK, 0, c->stream>>>(a, 0);
     DCU_LAUNCHED(c, "k_bi_true");
   }

@@ -700,10 +700,10 @@ int dcu_batch_solve_d(dcu_spai_ctx* c, int nsys, const int* sys_off, int n, int 
   }
 }
 
-int dcu_sell_plan_stats(dcu_spai_ctx* c, long long* slots, long long* uniform_slots) {
+int dcu_sell_plan_stats(dcu_spai_ctx* c, long long* slots, long long* uniform_slots, long long* wide_slices) {
   if (!c) return DCU_ERR_ARG;
   StreamScope scope(c);
-  return dcu::plan_stats(c, slots, uniform_slots);
+  return dcu::plan_stats(c, slots, uniform_slots, wide_slices);
 }
 
 int dcu_profile_iteration_kernels(dcu_spai_ctx* c, int reps, float* ms_out, int cap, int* count) {

@@ -55,6 +55,8 @@ enum BufId {
   B_HUBPOOL,       // slabs of the columns factored by the hub kernels
   B_HUBMETA,       // their descriptors
   B_HUBWPRE,       // prefix of their widths (warp -> column map)
+  B_SELL_WIDE,     // SELL: count and list of the slices wider than kWideSlice
+  B_WIDEVAL,       // solver: row values of those slices, from the wide pre-pass
   B_COUNT
 };
 
@@ -106,6 +108,7 @@ struct Ctx {
   std::vector<int> profile_sel;    // and the grid selector each ran with
   bool profile_k1_free = false;    // fused and split first steps compute the same values
   int profile_default_split = 0;   // the form's default first step
+  int plan_wide = 0;               // slices of the last SELL plan wider than kWideSlice
 };
 
 // Iteration kernels of BiCGSTAB, for profiling and the autotuner.
@@ -148,6 +151,10 @@ int scan_exclusive_i64(Ctx* c, const int* in, long long* out, int n);
 // ---------------------------------------------------------------------------
 // Sparse pattern analysis of A (CSC): CSR transpose and SELL-32 layout.
 // ---------------------------------------------------------------------------
+// A full slice wider than this many slots (a row that long shares its slice
+// with 31 others) is summed by a warp-cooperative pre-pass in the solver.
+constexpr int kWideSlice = 64;
+
 struct SellPlan {
   int n = 0, nnz = 0;
   int nslices = 0;
@@ -162,11 +169,17 @@ struct SellPlan {
   // row of the slice has its k-th entry at column row + d, else 0.  A warp
   // then forms the column from the row and skips the per-slot index load.
   const int* kd = nullptr;
-  const int* su = nullptr;  // per slice: 1 when every kd of the slice is uniform
+  // Per slice: bit 0 when every kd of the slice is uniform; bit 2 when the
+  // slice is full and wider than kWideSlice, with its index in `wide` in the
+  // bits above bit 2.
+  const int* su = nullptr;
+  const int* rptr = nullptr;  // CSR row pointers of the laid-out operator (row lengths)
+  const int* wide = nullptr;  // slices wider than kWideSlice (device)
+  int nwide = 0;
 };
 
 // Slot counts of the last SELL plan built on a context (diagnostics).
-int plan_stats(Ctx* c, long long* slots, long long* uniform_slots);
+int plan_stats(Ctx* c, long long* slots, long long* uniform_slots, long long* wide_slices);
 
 // Fails with DCU_ERR_ARG unless ptr[0] = 0, ptr is non-decreasing,
 // ptr[n] = nnz and every row index lies in [0, n).  Every entry point runs it

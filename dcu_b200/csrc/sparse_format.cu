@@ -292,7 +292,8 @@ __global__ void k_sell_delta(const int* __restrict__ sidx, long long slots, int 
 // count.  Writes kd[off[s] / 32 + k] = (d << 1) | 1, or 0, and su[s] = 1 when
 // every k of the slice has one offset (the SpMV then reads no index at all).
 __global__ void k_sell_desc(const int* __restrict__ sidx, int n, int nslices, const long long* __restrict__ off,
-                            int* __restrict__ kd, int* __restrict__ su, unsigned long long* __restrict__ uslots) {
+                            int* __restrict__ kd, int* __restrict__ su, unsigned long long* __restrict__ uslots,
+                            int* __restrict__ wide) {
   const int rows_total = nslices * 32;
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows_total; r += gridDim.x * blockDim.x) {
     const int s = r >> 5, lane = r & 31;
@@ -307,7 +308,15 @@ __global__ void k_sell_desc(const int* __restrict__ sidx, int n, int nslices, co
       if (lane == 0) kd[(o0 >> 5) + k] = same ? (int)(((unsigned)d0 << 1) | 1u) : 0;
     }
     if (lane == 0) {
-      su[s] = all ? 1 : 0;
+      int f = all ? 1 : 0;
+      // a full slice wider than kWideSlice: listed for the solver's pre-pass
+      // (wide[0] counts, wide[1 + i] = slice)
+      if (w > kWideSlice && 32 * s + 32 <= n) {
+        const int i = atomicAdd(wide, 1);
+        wide[1 + i] = s;
+        f |= 4 | (i << 3);
+      }
+      su[s] = f;
       if (all && w > 0) atomicAdd(uslots, 32ull * (unsigned long long)w);
     }
   }
@@ -503,9 +512,18 @@ int sell_fill_from_csr(Ctx* c, int n, int nnz, const int* rptr, const int* rcol,
   unsigned long long* pst = bp<unsigned long long>(c, B_PLANSTAT);
   const unsigned long long hst[2] = {(unsigned long long)slots, 0ull};
   DCU_CUDA(c, cudaMemcpyAsync(pst, hst, sizeof(hst), cudaMemcpyHostToDevice, c->stream));
+  DCU_TRY(ensure(c, B_SELL_WIDE, sizeof(int) * ((size_t)nslices + 1)));
+  int* wide = bp<int>(c, B_SELL_WIDE);
+  DCU_CUDA(c, cudaMemsetAsync(wide, 0, sizeof(int), c->stream));
   k_sell_desc<<<waves_grid(c, (long long)nslices * 32, 256, 8), 256, 0, c->stream>>>(sidx, n, nslices, off, kd, su,
-                                                                                       pst + 1);
+                                                                                       pst + 1, wide);
   DCU_LAUNCHED(c, "k_sell_desc");
+  DCU_CUDA(c, cudaMemcpyAsync(c->pinned, wide, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  DCU_CUDA(c, cudaStreamSynchronize(c->stream));
+  plan->nwide = *reinterpret_cast<int*>(c->pinned);
+  c->plan_wide = plan->nwide;
+  plan->wide = wide + 1;
+  plan->rptr = rptr;
   plan->kd = kd;
   plan->su = su;
   plan->n = n;
@@ -533,13 +551,14 @@ int sell_plan_rows(Ctx* c, int n, int nnz, const int* rptr, const int* rcol, Sel
   return sell_fill_from_csr(c, n, nnz, rptr, rcol, rperm, plan);
 }
 
-int plan_stats(Ctx* c, long long* slots, long long* uniform_slots) {
+int plan_stats(Ctx* c, long long* slots, long long* uniform_slots, long long* wide_slices) {
   if (!c->buf[B_PLANSTAT].p) return fail(c, DCU_ERR_ARG, "no SELL plan has been built on this context");
   unsigned long long h[2] = {0, 0};
   DCU_CUDA(c, cudaMemcpyAsync(h, c->buf[B_PLANSTAT].p, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
   DCU_CUDA(c, cudaStreamSynchronize(c->stream));
   if (slots) *slots = (long long)h[0];
   if (uniform_slots) *uniform_slots = (long long)h[1];
+  if (wide_slices) *wide_slices = c->plan_wide;
   return DCU_OK;
 }
 

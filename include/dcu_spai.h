@@ -282,9 +282,11 @@ int dcu_profile_iteration_kernels(dcu_spai_ctx* ctx, int reps, float* ms_out, in
 /* Diagnostics of the last SELL-32 layout built on this context (by any solve
  * that runs BiCGSTAB): *slots = slots including padding, *uniform_slots =
  * slots in slices whose every entry position has one column offset for all
- * 32 rows (those slices read no index array).  Either output may be NULL.
- * No counterpart in the reference. */
-int dcu_sell_plan_stats(dcu_spai_ctx* ctx, long long* slots, long long* uniform_slots);
+ * 32 rows (those slices read no index array), *wide_slices = full slices
+ * wider than 64 slots (a long row), whose rows a warp-cooperative pre-pass
+ * sums before each SpMV.  Any output may be NULL.  No counterpart in the
+ * reference. */
+int dcu_sell_plan_stats(dcu_spai_ctx* ctx, long long* slots, long long* uniform_slots, long long* wide_slices);
 
 /* ---- autotuner (no counterpart in the reference) ----------------------------- */
 

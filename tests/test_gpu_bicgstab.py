@@ -165,12 +165,15 @@ def test_sell_plan_stats_and_offset_aligned_slices(ctx):
     where row + offset leaves the matrix; an irregular matrix mostly does not.
     Both solve to the same iterations as the oracle (the layout only moves
     zeros around)."""
-    for A, lo, hi in ((W.convdiff3d(16, 20.0), 0.95, 1.0), (W.circuit_like(), 0.0, 0.9)):
+    for A, lo, hi, wide in ((W.convdiff3d(16, 20.0), 0.95, 1.0, False), (W.circuit_like(), 0.0, 0.9, True)):
         b, _ = W.rhs_from_solution(A, seed=2)
         x, _, _, si = ctx.solve_h(A, b, precision=N.PREC_FP64)
-        slots, uni = ctx.sell_plan_stats()
+        slots, uni, nwide = ctx.sell_plan_stats(wide=True)
         assert slots >= A.nnz and 0 <= uni <= slots
         assert lo <= uni / slots <= hi, (uni, slots)
+        # the hub rows of the circuit-like matrix (200-400 entries) make their
+        # slices wide: summed by the warp-cooperative pre-pass
+        assert (nwide > 0) == wide, nwide
         m_o, _, _, _ = oracle.spai(A, "mgs")
         ref = oracle.bicgstab(A, m_o, b, None, tol=1e-8, tol_mode="rel", maxiter=1000)
         assert si.status == N.SOLVE_CONVERGED and abs(si.iters - ref["iters"]) <= 1
