@@ -11,8 +11,8 @@ Synthetic seeded data; the reference publishes no number for it.
          deltas, FP64 Krylov vectors) with A, b resident in HBM
   e2e    the same through the host-buffer C entry point dcu_spai_solve_h:
          pinned host A, b, x0 -> device, solve, x -> host, per step
-  plain_fp64_ms  the plain FP64 form on the same inputs (the north star's
-         comparison), measured in the same run
+  plain_fp64_ms  the plain FP64 form on the same inputs (the form the mixed
+         precision forms are compared with), measured in the same run
 
 python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                 [--workload cd3d128|batch512|grad512]

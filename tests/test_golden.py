@@ -46,7 +46,7 @@ def test_oracle_reproduces_golden(name):
     assert ref["iters"] == g["iters_reference_settings"]
 
 
-def test_survey_reference_algorithm_facts():
+def test_reference_algorithm_facts():
     # 64x64 Pe 10: 43 iterations with the reference's solver settings, 45 with
     # the config's (b = A 1, x0 = 0, relative 1e-8)
     g = GOLDEN["convdiff2d_64_pe10"]
