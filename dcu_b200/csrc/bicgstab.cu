@@ -66,8 +66,9 @@ __device__ __forceinline__ double ldv(const T* p) { return (double)__ldg(p); }
 // keeps up to 16 independent loads in flight.  A slice whose every k has one
 // column offset for all its rows (su[s]; SellPlan::kd) reads no index at all:
 // the column is the row plus the slice's offset, one broadcast load per k
-// from a table 1/32 the size of the index array.  The rows of a slice wider
-// than kWideSlice were summed by the wide pre-pass (k_bi_wide) into wv.
+// from a table 1/32 the size of the index array.  The rows of a slice that
+// the plan flagged wide (su bit 2) were summed by the wide pre-pass
+// (k_bi_wide) into wv.
 template <typename MT, typename IT, typename F>
 __device__ __forceinline__ double sell_row(const long long* __restrict__ off, const int* __restrict__ kd,
                                            const int* __restrict__ su, const double* __restrict__ wv,
@@ -208,8 +209,8 @@ __device__ __forceinline__ bool finished(const Scal* S) {
 __device__ __forceinline__ bool bad(double v) { return !isfinite(v); }
 
 // ---- wide pre-pass ---------------------------------------------------------
-// A full slice wider than kWideSlice holds a long row; in sell_row its warp
-// would walk every slot of the slice, with one gather latency per 8 slots.
+// A full slice made wider than kWideSlice by a few long rows; in sell_row its
+// warp would walk every slot of the slice, with one gather latency per 8 slots.
 // Here a warp takes one such slice: each lane sums its own row up to its own
 // length (rptr), 8 slots at a time as in sell_row; then the rows longer than
 // kWideSlice are summed one at a time by the whole warp, each lane loading one

@@ -151,9 +151,12 @@ int scan_exclusive_i64(Ctx* c, const int* in, long long* out, int n);
 // ---------------------------------------------------------------------------
 // Sparse pattern analysis of A (CSC): CSR transpose and SELL-32 layout.
 // ---------------------------------------------------------------------------
-// A full slice wider than this many slots (a row that long shares its slice
-// with 31 others) is summed by a warp-cooperative pre-pass in the solver.
-constexpr int kWideSlice = 64;
+// A full slice wider than kWideSlice slots because of at most kWideRows long
+// rows (a long row sharing its slice with short ones) is summed by a warp-
+// cooperative pre-pass in the solver.  Slices where more rows are that long
+// keep the per-lane loop, which serves them better.
+constexpr int kWideSlice = 32;
+constexpr int kWideRows = 4;
 
 struct SellPlan {
   int n = 0, nnz = 0;
@@ -170,11 +173,11 @@ struct SellPlan {
   // then forms the column from the row and skips the per-slot index load.
   const int* kd = nullptr;
   // Per slice: bit 0 when every kd of the slice is uniform; bit 2 when the
-  // slice is full and wider than kWideSlice, with its index in `wide` in the
-  // bits above bit 2.
+  // slice is full, wider than kWideSlice and has at most kWideRows rows
+  // longer than that, with its index in `wide` in the bits above bit 2.
   const int* su = nullptr;
   const int* rptr = nullptr;  // CSR row pointers of the laid-out operator (row lengths)
-  const int* wide = nullptr;  // slices wider than kWideSlice (device)
+  const int* wide = nullptr;  // the slices flagged wide (device)
   int nwide = 0;
 };
 

@@ -293,7 +293,7 @@ __global__ void k_sell_delta(const int* __restrict__ sidx, long long slots, int 
 // every k of the slice has one offset (the SpMV then reads no index at all).
 __global__ void k_sell_desc(const int* __restrict__ sidx, int n, int nslices, const long long* __restrict__ off,
                             int* __restrict__ kd, int* __restrict__ su, unsigned long long* __restrict__ uslots,
-                            int* __restrict__ wide) {
+                            const int* __restrict__ rptr, int* __restrict__ wide) {
   const int rows_total = nslices * 32;
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows_total; r += gridDim.x * blockDim.x) {
     const int s = r >> 5, lane = r & 31;
@@ -307,11 +307,14 @@ __global__ void k_sell_desc(const int* __restrict__ sidx, int n, int nslices, co
       all = all && same;
       if (lane == 0) kd[(o0 >> 5) + k] = same ? (int)(((unsigned)d0 << 1) | 1u) : 0;
     }
+    // rows of the slice longer than kWideSlice
+    const int len = (r < n) ? rptr[r + 1] - rptr[r] : 0;
+    const int nlong = __popc(__ballot_sync(0xffffffffu, len > kWideSlice));
     if (lane == 0) {
       int f = all ? 1 : 0;
-      // a full slice wider than kWideSlice: listed for the solver's pre-pass
-      // (wide[0] counts, wide[1 + i] = slice)
-      if (w > kWideSlice && 32 * s + 32 <= n) {
+      // a full slice made wide by a few long rows: listed for the solver's
+      // pre-pass (wide[0] counts, wide[1 + i] = slice)
+      if (w > kWideSlice && nlong <= kWideRows && 32 * s + 32 <= n) {
         const int i = atomicAdd(wide, 1);
         wide[1 + i] = s;
         f |= 4 | (i << 3);
@@ -516,7 +519,7 @@ int sell_fill_from_csr(Ctx* c, int n, int nnz, const int* rptr, const int* rcol,
   int* wide = bp<int>(c, B_SELL_WIDE);
   DCU_CUDA(c, cudaMemsetAsync(wide, 0, sizeof(int), c->stream));
   k_sell_desc<<<waves_grid(c, (long long)nslices * 32, 256, 8), 256, 0, c->stream>>>(sidx, n, nslices, off, kd, su,
-                                                                                       pst + 1, wide);
+                                                                                       pst + 1, rptr, wide);
   DCU_LAUNCHED(c, "k_sell_desc");
   DCU_CUDA(c, cudaMemcpyAsync(c->pinned, wide, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   DCU_CUDA(c, cudaStreamSynchronize(c->stream));
