@@ -158,7 +158,7 @@ class Context:
 
     def sell_plan_stats(self, wide: bool = False):
         """(slots, uniform_slots) of the last SELL layout built on this context; with wide=True also the
-        number of full slices made wider than 32 slots by at most 4 long rows (summed by the warp-cooperative
+        number of full slices made wider than 16 slots by at most 4 long rows (summed by the warp-cooperative
         pre-pass)."""
         s, u, w = C.c_longlong(), C.c_longlong(), C.c_longlong()
         self._check(self._L.dcu_sell_plan_stats(self.h, C.byref(s), C.byref(u), C.byref(w)))

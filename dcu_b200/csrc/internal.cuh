@@ -155,7 +155,7 @@ int scan_exclusive_i64(Ctx* c, const int* in, long long* out, int n);
 // rows (a long row sharing its slice with short ones) is summed by a warp-
 // cooperative pre-pass in the solver.  Slices where more rows are that long
 // keep the per-lane loop, which serves them better.
-constexpr int kWideSlice = 32;
+constexpr int kWideSlice = 16;
 constexpr int kWideRows = 4;
 
 struct SellPlan {

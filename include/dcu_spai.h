@@ -283,7 +283,7 @@ int dcu_profile_iteration_kernels(dcu_spai_ctx* ctx, int reps, float* ms_out, in
  * that runs BiCGSTAB): *slots = slots including padding, *uniform_slots =
  * slots in slices whose every entry position has one column offset for all
  * 32 rows (those slices read no index array), *wide_slices = full slices
- * wider than 32 slots because of at most 4 longer rows, whose rows a
+ * wider than 16 slots because of at most 4 longer rows, whose rows a
  * warp-cooperative pre-pass sums before each SpMV.  Any output may be NULL.  No counterpart in the
  * reference. */
 int dcu_sell_plan_stats(dcu_spai_ctx* ctx, long long* slots, long long* uniform_slots, long long* wide_slices);

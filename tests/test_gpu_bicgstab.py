@@ -171,8 +171,9 @@ def test_sell_plan_stats_and_offset_aligned_slices(ctx):
         slots, uni, nwide = ctx.sell_plan_stats(wide=True)
         assert slots >= A.nnz and 0 <= uni <= slots
         assert lo <= uni / slots <= hi, (uni, slots)
-        # the hub rows of the circuit-like matrix (200-400 entries) make their
-        # slices wide: summed by the warp-cooperative pre-pass
+        # the long rows of the circuit-like matrix (hubs of 200-400 entries,
+        # power-law degrees) make their slices wide: summed by the
+        # warp-cooperative pre-pass
         assert (nwide > 0) == wide, nwide
         m_o, _, _, _ = oracle.spai(A, "mgs")
         ref = oracle.bicgstab(A, m_o, b, None, tol=1e-8, tol_mode="rel", maxiter=1000)
