@@ -214,7 +214,7 @@ __device__ __forceinline__ bool bad(double v) { return !isfinite(v); }
 // Here a warp takes one such slice: each lane sums its own row up to its own
 // length (rptr), 8 slots at a time as in sell_row; then the rows longer than
 // kWideSlice are summed one at a time by the whole warp, each lane loading one
-// entry in 32 and its gather (the next 32 prefetched), and one chain of
+// entry in 32 and its gather (two chunks of 32 prefetched), and one chain of
 // multiply-adds consuming them in k order through shuffles.  Every row's sum
 // is formed in sell_row's order with its operations, stopping at the row's
 // length instead of running over the zero padding, so the iterates do not
@@ -265,11 +265,13 @@ __device__ __forceinline__ double wide_row(long long o0, const int* __restrict__
         xv = 0.0;
       }
     };
-    double chain = 0.0, av0, xv0;
+    // two chunks in flight ahead of the one being consumed
+    double chain = 0.0, av0, xv0, av1, xv1;
     load(lane, av0, xv0);
+    load(32 + lane, av1, xv1);
     for (int c0 = 0; c0 < lj; c0 += 32) {
-      double av1, xv1;
-      load(c0 + 32 + lane, av1, xv1);
+      double av2, xv2;
+      load(c0 + 64 + lane, av2, xv2);
       const int cnt = min(32, lj - c0);
       for (int t = 0; t < cnt; ++t) {
         const double at = __shfl_sync(0xffffffffu, av0, t);
@@ -278,6 +280,8 @@ __device__ __forceinline__ double wide_row(long long o0, const int* __restrict__
       }
       av0 = av1;
       xv0 = xv1;
+      av1 = av2;
+      xv1 = xv2;
     }
     if (lane == j) acc = chain;
   }
