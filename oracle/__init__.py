@@ -6,7 +6,12 @@ never imports it.
 
 ``ref_*`` helpers wrap oracle/_ref/libref_harness.so, the reference's own CPU
 helpers compiled from the reference tree; they exist only where that tree was
-present at build time.
+present at build time.  ``fixture_path`` finds the reference's MatrixMarket
+fixtures: the copies the build staged in oracle/_ref/matrices (they travel with
+the built files), else the reference tree itself.
+
+The reference tree is found at $DCU_REFERENCE, else at the recipe's default
+(oracle/Makefile).
 """
 from __future__ import annotations
 
@@ -17,19 +22,35 @@ import subprocess
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
+REFERENCE = os.environ.get("DCU_REFERENCE", "/root/reference")
 _LIB = None
 _REF = None
+_EMU = None
 
 _i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 _i64p = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 
 
-def build(reference: str | None = "/root/reference") -> None:
-    """Compile liboracle.so (and the reference harness when the tree exists)."""
+def reference_present() -> bool:
+    return os.path.isdir(os.path.join(REFERENCE, "include", "common"))
+
+
+def build(reference: str | None = REFERENCE) -> None:
+    """Compile liboracle.so (and, when the reference tree exists, the harness
+    over its CPU helpers plus the staged copies of its fixtures)."""
     subprocess.run(["make", "-s", "-C", _HERE, "all"], check=True)
     if reference and os.path.isdir(os.path.join(reference, "include", "common")):
-        subprocess.run(["make", "-s", "-C", _HERE, "ref", f"REFERENCE={reference}"], check=True)
+        subprocess.run(["make", "-s", "-C", _HERE, "ref", "emu", f"REFERENCE={reference}"], check=True)
+
+
+def fixture_path(name: str) -> str | None:
+    """Path of the reference fixture matrices/<name>, or None when neither the
+    staged copy nor the reference tree has it."""
+    for p in (os.path.join(_HERE, "_ref", "matrices", name), os.path.join(REFERENCE, "matrices", name)):
+        if os.path.exists(p):
+            return p
+    return None
 
 
 def lib():
@@ -73,6 +94,8 @@ def ref():
                                C.POINTER(C.POINTER(C.c_double))]
         L.ref_n1max.restype = C.c_int
         L.ref_n1max.argtypes = [C.c_int, _i32p, _i32p, _f64p]
+        L.ref_n1_per_column.restype = None
+        L.ref_n1_per_column.argtypes = [C.c_int, _i32p, _i32p, _f64p, C.c_int, C.c_int, _i32p]
         L.ref_n2max.restype = C.c_int
         L.ref_n2max.argtypes = [C.c_int, _i32p, _i32p, _f64p]
         L.ref_csc2csr.restype = None
@@ -82,8 +105,49 @@ def ref():
     return _REF
 
 
+def emu_available() -> bool:
+    return os.path.exists(os.path.join(_HERE, "_ref", "libref_emu.so"))
+
+
+def emu():
+    """oracle/_ref/libref_emu.so: the reference's own SPAI kernels on the host
+    SIMT emulator and its BiCGSTAB over host stand-ins (ref_emulate.cpp)."""
+    global _EMU
+    if _EMU is None:
+        L = C.CDLL(os.path.join(_HERE, "_ref", "libref_emu.so"))
+        L.refemu_spai.restype = C.c_int
+        L.refemu_spai.argtypes = [C.c_int, _i32p, _i32p, _f64p, _f64p, C.c_longlong, _i32p]
+        L.refemu_bicgstab.restype = C.c_int
+        L.refemu_bicgstab.argtypes = [C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p, _f64p, C.c_double, C.c_int,
+                                      C.POINTER(C.c_double)]
+        _EMU = L
+    return _EMU
+
+
 def _c(a, dt):
     return np.ascontiguousarray(a, dtype=dt)
+
+
+def refemu_spai(A, tile_budget_bytes: int = 1 << 30):
+    """M's values from the reference's own kernels: (mval[nnz], info) with
+    info = (n1max, n2max, tiles, single_pass)."""
+    mval = np.zeros(max(1, A.nnz), dtype=np.float64)
+    info = np.zeros(4, dtype=np.int32)
+    rc = emu().refemu_spai(A.n, _c(A.ptr, np.int32), _c(A.idx, np.int32), _c(A.val, np.float64), mval,
+                           int(tile_budget_bytes), info)
+    if rc != 0:
+        raise RuntimeError(f"refemu_spai failed: {rc}")
+    return mval[: A.nnz], tuple(int(v) for v in info)
+
+
+def refemu_bicgstab(A, mval, b, x0, tol: float, maxiter: int):
+    """The reference's cublas2_pbicgstabv2 (absolute ||r|| < tol, counter as
+    the reference's): dict(iters, x, res)."""
+    x = np.array(x0, dtype=np.float64, copy=True)
+    err = C.c_double()
+    it = emu().refemu_bicgstab(A.n, _c(A.ptr, np.int32), _c(A.idx, np.int32), _c(A.val, np.float64),
+                               _c(mval, np.float64), _c(b, np.float64), x, float(tol), int(maxiter), C.byref(err))
+    return dict(iters=int(it), x=x, res=err.value)
 
 
 def set_threads(t: int) -> None:
@@ -182,6 +246,15 @@ def ref_mtx_read(path: str):
 
 def ref_n1max(A) -> int:
     return int(ref().ref_n1max(A.n, _c(A.ptr, np.int32), _c(A.idx, np.int32), _c(A.val, np.float64)))
+
+
+def ref_n1_per_column(A, col_start: int = 0, col_end: int | None = None):
+    """|I_k| of each column from the reference's computeN1MAX on a one-column M."""
+    col_end = A.n if col_end is None else col_end
+    out = np.zeros(max(1, col_end - col_start), dtype=np.int32)
+    ref().ref_n1_per_column(A.n, _c(A.ptr, np.int32), _c(A.idx, np.int32), _c(A.val, np.float64),
+                            col_start, col_end, out)
+    return out[: col_end - col_start]
 
 
 def ref_n2max(A) -> int:

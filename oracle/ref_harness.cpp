@@ -6,7 +6,8 @@
 //
 // Wrapped reference functions:
 //   readMatrixToCSC   include/common/read.h:1296-1320
-//   computeN1MAX      include/common/init.h:43-75
+//   computeN1MAX      include/common/init.h:43-75 (whole matrix: max |I_k|;
+//                     one-column M per call: |I_k| of every column)
 //   computeN2MAX      include/common/init.h:80-92
 //   CSC2CSR           include/common/assemble.h:34-67
 #include <cctype>
@@ -70,6 +71,31 @@ int ref_n1max(int n, int* ptr, int* idx, double* val) {
   A.mIndex = idx;
   A.mData = val;
   return computeN1MAX(&A, &A);
+}
+
+// |I_k| of every column k in [c0, c1), each from computeN1MAX called on a
+// one-column M whose only column holds J_k = the rows of A(:, k)
+// (mPtr = {0, |J_k|}, mIndex = A's indices of column k).  The reference
+// function keeps its own vector per call, so columns run in parallel.
+void ref_n1_per_column(int n, int* ptr, int* idx, double* val, int c0, int c1, int* out) {
+  CSC_Matrix A;
+  A.n = A.nRow = A.nCol = n;
+  A.nonzeroes = ptr[n];
+  A.mPtr = ptr;
+  A.mIndex = idx;
+  A.mData = val;
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int k = c0; k < c1; ++k) {
+    int mp[2] = {0, ptr[k + 1] - ptr[k]};
+    CSC_Matrix M;
+    M.n = M.nCol = 1;
+    M.nRow = n;
+    M.nonzeroes = mp[1];
+    M.mPtr = mp;
+    M.mIndex = idx + ptr[k];
+    M.mData = val + ptr[k];
+    out[k - c0] = computeN1MAX(&A, &M);
+  }
 }
 
 int ref_n2max(int n, int* ptr, int* idx, double* val) {

@@ -7,7 +7,6 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-REFERENCE = "/root/reference"
 
 
 def pytest_configure(config):
@@ -20,10 +19,10 @@ def _built():
     from dcu_b200 import build as B
     import oracle
 
-    if not os.path.exists(B.LIBNAME) or not os.path.exists(B.CLINAME):
+    if not all(os.path.exists(p) for p in (B.LIBNAME, B.CLINAME, B.CLI_SINGLE)):
         B.build()
     if not os.path.exists(os.path.join(ROOT, "oracle", "liboracle.so")):
-        oracle.build(REFERENCE if os.path.isdir(REFERENCE) else None)
+        oracle.build(oracle.REFERENCE if oracle.reference_present() else None)
     yield
 
 
@@ -37,7 +36,11 @@ def ctx():
 
 
 def reference_file(rel):
-    p = os.path.join(REFERENCE, rel)
-    if not os.path.exists(p):
-        pytest.skip(f"reference tree not present ({rel})")
+    """A reference fixture ("matrices/<name>"): the copy staged with the built
+    oracle files, else the reference tree; skip when neither has it."""
+    import oracle
+
+    p = oracle.fixture_path(os.path.basename(rel))
+    if p is None:
+        pytest.skip(f"reference fixture not present ({rel})")
     return p

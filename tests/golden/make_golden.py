@@ -1,6 +1,15 @@
 """Regenerate tests/golden/golden.json from the CPU oracle (and, where the
-reference tree is present, from the reference's own CPU helpers and its
-MatrixMarket fixture).  Run: python tests/golden/make_golden.py"""
+reference tree is present, from the reference's own CPU helpers and its two
+MatrixMarket fixtures).  Run: python tests/golden/make_golden.py
+(the MGS build of circuit_2.mtx takes a few minutes); with --sensitivity it
+writes tests/golden/sensitivity.json instead (see sensitivity()).
+
+Per fixture it records the file's SHA-256 (the GPU tests check that the copy
+they read is the reference's file), the reader's CSC digests, |I_k| of every
+column from the reference's computeN1MAX, and the oracle's SPAI/BiCGSTAB
+results in the reference's solver settings (b = 1, x0 = 1, ||r|| < 1e-7
+absolute, MAX_ITER 10000) and in the configs' (b = A 1, x0 = 0, relative
+1e-8, maxiter 1000)."""
 import hashlib
 import json
 import os
@@ -14,7 +23,6 @@ sys.path.insert(0, ROOT)
 import oracle  # noqa: E402
 from dcu_b200 import workloads as W  # noqa: E402
 
-REF = "/root/reference"
 
 
 def digest(a):
@@ -42,22 +50,104 @@ def case(name, A, b_kind):
     return out
 
 
+def file_sha256(path):
+    with open(path, "rb") as f:
+        return hashlib.sha256(f.read()).hexdigest()
+
+
+def fixture(path):
+    A = oracle.ref_mtx_read(path)
+    cnt, _, il = oracle.pattern(A)
+    icount_ref = oracle.ref_n1_per_column(A)
+    assert np.array_equal(cnt, icount_ref)
+    m, colres, E, sing = oracle.spai(A, "mgs")
+    out = {"file_sha256": file_sha256(path), "n": A.n, "nnz": A.nnz, "ptr_sha": digest(A.ptr),
+           "idx_sha": digest(A.idx), "val_sha": digest(A.val), "icount_reference_sha": digest(icount_ref),
+           "pattern_sha": digest(il), "max_ni": int(cnt.max()), "max_nj": int(np.diff(A.ptr).max()),
+           "m_sum": float(m.sum()), "m_sumsq": float((m * m).sum()), "colres_max": float(colres.max()),
+           "singular": sing, "diag_missing": int(A.n - sum(1 for k in range(A.n)
+                                                           if k in A.idx[A.ptr[k]:A.ptr[k + 1]]))}
+    r = oracle.bicgstab(A, m, np.ones(A.n), np.ones(A.n), tol=1e-7, tol_mode="abs", maxiter=10000)
+    out["reference_settings"] = {"iters": r["iters"], "status": r["status"], "res": r["res"]}
+    b = W.rhs_ones_product(A)
+    r = oracle.bicgstab(A, m, b, None, tol=1e-8, tol_mode="rel", maxiter=1000)
+    out["config_settings"] = {"iters": r["iters"], "status": r["status"],
+                              "rel_res": r["true_res"] / float(np.linalg.norm(b))}
+    return out
+
+
 def main():
     g = {
         "convdiff2d_64_pe10": case("cd2d", W.convdiff2d(64, 10.0), "ones_product"),
         "convdiff3d_16_pe20": case("cd3d", W.convdiff3d(16, 20.0), "solution"),
         "circuit_like_seed2024": case("circuit", W.circuit_like(), "uniform"),
     }
-    path = os.path.join(REF, "matrices", "circuit_2.mtx")
-    if os.path.exists(path) and oracle.ref_available():
+    path = oracle.fixture_path("circuit_2.mtx")
+    if path and oracle.ref_available():
         A = oracle.ref_mtx_read(path)
         cnt, _, il = oracle.pattern(A)
         g["circuit_2_mtx"] = {"n": A.n, "nnz": A.nnz, "ptr_sha": digest(A.ptr), "idx_sha": digest(A.idx),
                               "val_sha": digest(A.val), "n1max_reference": oracle.ref_n1max(A),
                               "n2max_reference": oracle.ref_n2max(A), "pattern_sha": digest(il)}
+    fx = {}
+    for name in ("circuit_2.mtx", "fill_3elt.mtx"):
+        path = oracle.fixture_path(name)
+        if path and oracle.ref_available():
+            fx[name] = fixture(path)
+    if fx:
+        g["fixtures"] = fx
     with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden.json"), "w") as f:
         json.dump(g, f, indent=1, sort_keys=True)
 
 
+def _perturbed(m, seed):
+    """M with every value moved by one unit in the last place, up or down at
+    random: a change below any summation-order difference."""
+    s = np.random.Generator(np.random.PCG64(seed)).integers(0, 2, m.size).astype(bool)
+    return np.where(s, np.nextafter(m, np.inf), np.nextafter(m, -np.inf))
+
+
+def sensitivity(trials=8):
+    """Spread of the oracle's own BiCGSTAB iteration count when M moves by one
+    ulp per value, on the benchmark workloads with long solves: the band a
+    solver with another summation order can be held to.  Writes
+    tests/golden/sensitivity.json."""
+    out = {}
+    A = W.varcoef2d(512, seed=5)
+    rng = np.random.Generator(np.random.PCG64(5))
+    b, xt = rng.standard_normal(A.n), rng.standard_normal(A.n)
+    m, _, _, _ = oracle.spai(A, "mgs")
+    base = oracle.bicgstab(A, m, b, None, tol=1e-8, tol_mode="rel", maxiter=3000)
+    g = 2.0 * (base["x"] - xt)
+    rp, ri, rv = oracle.csc2csr(A.n, A.ptr, A.idx, A.val)
+    At = W.CSC(A.n, rp, ri, rv)
+    fwd, adj = [], []
+    base_t = oracle.bicgstab(At, oracle.csc2csr(A.n, A.ptr, A.idx, m)[2], g, None, tol=1e-8, tol_mode="rel",
+                             maxiter=3000)
+    for t in range(1, trials + 1):
+        mp = _perturbed(m, t)
+        fwd.append(oracle.bicgstab(A, mp, b, None, tol=1e-8, tol_mode="rel", maxiter=3000)["iters"])
+        mt = oracle.csc2csr(A.n, A.ptr, A.idx, mp)[2]
+        adj.append(oracle.bicgstab(At, mt, g, None, tol=1e-8, tol_mode="rel", maxiter=3000)["iters"])
+    spread = lambda base_it, its: max(1, max(abs(v - base_it) for v in its))
+    out["varcoef512"] = {"forward_iters": base["iters"], "forward_perturbed": fwd,
+                         "forward_iters_band": spread(base["iters"], fwd),
+                         "adjoint_iters": base_t["iters"], "adjoint_perturbed": adj,
+                         "adjoint_iters_band": spread(base_t["iters"], adj), "trials": trials}
+    A = W.convdiff3d(128, 20.0)
+    b, _ = W.rhs_from_solution(A, seed=7)
+    m, _, _, _ = oracle.spai(A, "mgs")
+    base = oracle.bicgstab(A, m, b, None, tol=1e-8, tol_mode="rel", maxiter=1000)
+    its = [oracle.bicgstab(A, _perturbed(m, t), b, None, tol=1e-8, tol_mode="rel", maxiter=1000)["iters"]
+           for t in range(1, trials + 1)]
+    out["convdiff3d_128"] = {"iters": base["iters"], "perturbed": its, "iters_band": spread(base["iters"], its),
+                             "trials": trials}
+    with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "sensitivity.json"), "w") as f:
+        json.dump(out, f, indent=1, sort_keys=True)
+
+
 if __name__ == "__main__":
-    main()
+    if "--sensitivity" in sys.argv:
+        sensitivity()
+    else:
+        main()

@@ -55,8 +55,8 @@ def test_reference_algorithm_facts():
 
 
 def test_reader_matches_fixture_digests():
-    path = "/root/reference/matrices/circuit_2.mtx"
-    if not os.path.exists(path):
+    path = oracle.fixture_path("circuit_2.mtx")
+    if path is None:
         pytest.skip("reference fixture absent")
     from dcu_b200.api import mtx_read
 

@@ -1,9 +1,10 @@
 """Pins against the reference's own CPU code, compiled from the reference tree
-into oracle/_ref (skipped where that tree is absent, e.g. on the GPU box):
+into oracle/_ref (skipped where that harness was not built: no reference tree):
 
 * the library's MatrixMarket reader == readMatrixToCSC (read.h:1296-1320)
 * the oracle's CSC->CSR == CSC2CSR (assemble.h:34-67)
-* the oracle's max |I_k| / max |J_k| == computeN1MAX / computeN2MAX (init.h:43-92)
+* the oracle's max |I_k| / max |J_k| == computeN1MAX / computeN2MAX (init.h:43-92), and
+  |I_k| of every column == computeN1MAX on a one-column M holding J_k
 """
 import os
 
@@ -48,9 +49,9 @@ def test_reader_fixtures(rel):
 
 def _fixtures():
     out = [W.convdiff2d(32, 10.0), W.circuit_like(), W.varcoef2d(24, seed=1)]
-    for rel in ["matrices/circuit_2.mtx", "matrices/fill_3elt.mtx"]:
-        p = os.path.join("/root/reference", rel)
-        if os.path.exists(p):
+    for name in ["circuit_2.mtx", "fill_3elt.mtx"]:
+        p = oracle.fixture_path(name)
+        if p is not None:
             out.append(api.mtx_read(p))
     return out
 
@@ -76,3 +77,28 @@ def test_sizing_pinned(k):
     cnt, _, _ = oracle.pattern(A)
     assert int(cnt.max()) == oracle.ref_n1max(A)
     assert int(np.diff(A.ptr).max()) == oracle.ref_n2max(A)
+
+
+PER_COLUMN = {
+    "convdiff2d_64": lambda: W.convdiff2d(64, 10.0),
+    "circuit_like": lambda: W.circuit_like(),
+    "varcoef2d_512": lambda: W.varcoef2d(512, seed=5),
+    "convdiff3d_128": lambda: W.convdiff3d(128, 20.0),
+    "circuit_2.mtx": lambda: api.mtx_read(reference_file("matrices/circuit_2.mtx")),
+    "fill_3elt.mtx": lambda: api.mtx_read(reference_file("matrices/fill_3elt.mtx")),
+}
+
+
+@pytest.mark.parametrize("name", list(PER_COLUMN))
+def test_every_column_sizing_pinned(name):
+    """|I_k| of every column: the oracle's pattern pass == the reference's
+    computeN1MAX run on a one-column M holding J_k (init.h:43-75)."""
+    A = PER_COLUMN[name]()
+    cnt, _, _ = oracle.pattern(A)
+    assert np.array_equal(cnt, oracle.ref_n1_per_column(A))
+
+
+def test_column_range_sizing_pinned():
+    A = W.circuit_like()
+    cnt, _, _ = oracle.pattern(A, 1000, 3217)
+    assert np.array_equal(cnt, oracle.ref_n1_per_column(A, 1000, 3217))
