@@ -1,5 +1,6 @@
 """Build recipe of libdcu_spai.so (CUDA sm_100a + host C++) and the
-spai_multi_dcu command-line driver, in-tree under dcu_b200/lib/.
+spai_multi_dcu and spai_single_dcu command-line drivers, in-tree under
+dcu_b200/lib/.
 
 nvcc compiles every kernel file for sm_100a only
 (-gencode arch=compute_100a,code=sm_100a); the host C++ (drop-in API,
@@ -20,6 +21,7 @@ OBJDIR = os.path.join(ROOT, "_build", "obj")
 INCLUDE = os.path.join(ROOT, "include")
 LIBNAME = os.path.join(LIBDIR, "libdcu_spai.so")
 CLINAME = os.path.join(LIBDIR, "spai_multi_dcu")
+CLI_SINGLE = os.path.join(LIBDIR, "spai_single_dcu")
 
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
@@ -83,11 +85,12 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
     if force or jobs or _stale(LIBNAME, objs):
         _run([NVCC, "-ccbin", HOST_CXX, *ARCH, "-shared", "-o", LIBNAME, *objs, "-Xlinker", "-z,defs",
               "-lpthread"])
-    cli_src = os.path.join(CSRC, "cli.cpp")
-    if force or _stale(CLINAME, [cli_src, LIBNAME] + hdrs):
-        _run([HOST_CXX, "-O2", "-std=c++17", "-I", INCLUDE, "-I", os.path.join(CUDA_HOME, "include"), cli_src,
-              "-o", CLINAME, "-L", LIBDIR, "-ldcu_spai", "-Wl,-rpath,$ORIGIN",
-              "-L", os.path.join(CUDA_HOME, "lib64"), "-lcudart"])
+    for src_name, exe in (("cli.cpp", CLINAME), ("cli_single.cpp", CLI_SINGLE)):
+        cli_src = os.path.join(CSRC, src_name)
+        if force or _stale(exe, [cli_src, LIBNAME] + hdrs):
+            _run([HOST_CXX, "-O2", "-std=c++17", "-Wall", "-I", INCLUDE, "-I", os.path.join(CUDA_HOME, "include"),
+                  cli_src, "-o", exe, "-L", LIBDIR, "-ldcu_spai", "-Wl,-rpath,$ORIGIN",
+                  "-L", os.path.join(CUDA_HOME, "lib64"), "-lcudart"])
     return LIBNAME
 
 

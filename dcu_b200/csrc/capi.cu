@@ -101,16 +101,19 @@ int solve_pipeline(Ctx* c, int n, int nnz, const int* ptr, const int* idx, const
   DCU_TRY(dcu::sell_plan(c, n, nnz, ptr, idx, &plan));
   if (val_ready) DCU_CUDA(c, cudaStreamWaitEvent(c->stream, val_ready, 0));
   dcu_build_info bl{};
-  DCU_CUDA(c, cudaEventRecord(c->ev[0], c->stream));
+  // the build's time is read after the solve's final synchronisation: no
+  // host round trip between the build and the solver's first launches
+  DCU_CUDA(c, cudaEventRecord(c->ev[4], c->stream));
   DCU_TRY(dcu::spai_build(c, n, nnz, ptr, idx, val, &o, m, nullptr, &bl));
-  DCU_CUDA(c, cudaEventRecord(c->ev[1], c->stream));
-  DCU_CUDA(c, cudaEventSynchronize(c->ev[1]));
-  cudaEventElapsedTime(&bl.ms, c->ev[0], c->ev[1]);
-  if (binfo) *binfo = bl;
+  DCU_CUDA(c, cudaEventRecord(c->ev[5], c->stream));
   const void* msell = nullptr;
   DCU_TRY(gather_values(c, plan, val, m, o.precision, &msell));
   if (bx_ready) DCU_CUDA(c, cudaStreamWaitEvent(c->stream, bx_ready, 0));
-  return dcu::bicgstab_solve(c, plan, dcu::bp<double>(c, dcu::B_SELL_AVAL), msell, b, x, &o, sinfo);
+  DCU_TRY(dcu::bicgstab_solve(c, plan, dcu::bp<double>(c, dcu::B_SELL_AVAL), msell, b, x, &o, sinfo));
+  DCU_CUDA(c, cudaEventSynchronize(c->ev[5]));
+  cudaEventElapsedTime(&bl.ms, c->ev[4], c->ev[5]);
+  if (binfo) *binfo = bl;
+  return DCU_OK;
 }
 
 // Host uploads share one buffer: ptr | idx | val | b | x | mval.
@@ -412,8 +415,8 @@ int dcu_spai_create(dcu_spai_ctx** out, int device, int units) {
     if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) { rc = dcu::cuda_fail(c, e, "stream", __FILE__, __LINE__); break; }
     if ((e = cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking)) != cudaSuccess) { rc = dcu::cuda_fail(c, e, "copy stream", __FILE__, __LINE__); break; }
     if ((e = cudaMallocHost(&c->pinned, dcu::kPinnedBytes)) != cudaSuccess) { rc = dcu::cuda_fail(c, e, "cudaMallocHost", __FILE__, __LINE__); break; }
-    for (int i = 0; i < 4 && e == cudaSuccess; ++i)
-      e = cudaEventCreateWithFlags(&c->ev[i], i < 2 ? cudaEventDefault : cudaEventDisableTiming);
+    for (int i = 0; i < 6 && e == cudaSuccess; ++i)
+      e = cudaEventCreateWithFlags(&c->ev[i], (i < 2 || i >= 4) ? cudaEventDefault : cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_sync, cudaEventDisableTiming);
     if (e != cudaSuccess) { rc = dcu::cuda_fail(c, e, "events", __FILE__, __LINE__); break; }
   } while (0);
@@ -567,7 +570,7 @@ int dcu_csc_to_csr_d(dcu_spai_ctx* c, int n, int nnz, const int* ptr, const int*
   if (rc) return rc;
   if (!rptr || (nnz > 0 && !ridx)) return dcu::fail(c, DCU_ERR_ARG, "null CSR output");
   StreamScope scope(c);
-  DCU_TRY(dcu::validate_csc(c, n, nnz, ptr, idx));
+  DCU_TRY(dcu::validate_csc(c, n, nnz, ptr, idx, /*unique_rows=*/false));
   DCU_TRY(dcu::ensure(c, dcu::B_RPERM, sizeof(int) * (size_t)(nnz > 0 ? nnz : 1)));
   int* perm = dcu::bp<int>(c, dcu::B_RPERM);
   DCU_TRY(dcu::csr_from_csc(c, n, nnz, ptr, idx, rptr, ridx, perm));
@@ -656,7 +659,7 @@ int dcu_sampled_outer_d(dcu_spai_ctx* c, int n, int nnz, const int* ptr, const i
   if (rc) return rc;
   if (!u || !v || (nnz > 0 && !out)) return dcu::fail(c, DCU_ERR_ARG, "null vector");
   StreamScope scope(c);
-  DCU_TRY(dcu::validate_csc(c, n, nnz, ptr, idx));
+  DCU_TRY(dcu::validate_csc(c, n, nnz, ptr, idx, /*unique_rows=*/false));
   DCU_TRY(dcu::sampled_outer(c, n, ptr, idx, u, v, alpha, out));
   DCU_CUDA(c, cudaStreamSynchronize(c->stream));
   return DCU_OK;

@@ -94,7 +94,10 @@ struct Ctx {
   long long launches = 0;
   DevBuf buf[B_COUNT];
   void* pinned = nullptr;   // small pinned host scratch (flags, stats), kPinnedBytes
-  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  // ev[0..1]: timing of one call's device work; ev[2..3]: the solver's
+  // stop-flag polling; ev[4..5]: the build inside a whole solve, read only
+  // after the solve's own final synchronisation
+  cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   std::vector<GraphSlot> graphs;  // BiCGSTAB iteration graphs (bounded cache)
   // launch configuration per precision form (dcu_set_tuning / dcu_autotune_d)
   dcu_tuning tune[5];
@@ -187,7 +190,10 @@ int plan_stats(Ctx* c, long long* slots, long long* uniform_slots, long long* wi
 // Fails with DCU_ERR_ARG unless ptr[0] = 0, ptr is non-decreasing,
 // ptr[n] = nnz and every row index lies in [0, n).  Every entry point runs it
 // before the first kernel that follows the indices.
-int validate_csc(Ctx* c, int n, int nnz, const int* ptr, const int* idx);
+// Structural check of a CSC matrix (status DCU_ERR_ARG with a message when it
+// fails).  unique_rows also refuses a row index repeated inside one column:
+// every SPAI and solver entry point needs distinct (row, column) pairs.
+int validate_csc(Ctx* c, int n, int nnz, const int* ptr, const int* idx, bool unique_rows = true);
 int csr_from_csc(Ctx* c, int n, int nnz, const int* ptr, const int* idx, int* rptr, int* rcol,
                  int* rperm);
 int csr_values(Ctx* c, int nnz, const int* rperm, const double* val, double* rval);

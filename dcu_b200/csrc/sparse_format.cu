@@ -353,7 +353,13 @@ int sell_gather(Ctx* c, const SellPlan& p, const double* src, T* dst) {
 }
 
 // Structural check of a CSC matrix before any kernel chases its indices:
-// ptr[0] == 0, ptr non-decreasing, ptr[n] == nnz, 0 <= idx < n.
+// ptr[0] == 0, ptr non-decreasing, ptr[n] == nnz, 0 <= idx < n.  One thread
+// per column walks that column's entries (only once its own bounds are known
+// to lie in [0, nnz]): a valid ptr partitions [0, nnz) into the columns, so
+// every entry is range-checked, and an invalid ptr is itself an error.  The
+// walk also compares neighbours: a repeated row in an ascending run is a
+// duplicate (32), a descent marks the matrix as having an unsorted column
+// (16), whose duplicates k_csc_duplicates then looks for.
 __global__ void k_validate_csc(const int* __restrict__ ptr, const int* __restrict__ idx, int n, int nnz,
                                int* __restrict__ bad) {
   const int stride = gridDim.x * blockDim.x;
@@ -362,13 +368,52 @@ __global__ void k_validate_csc(const int* __restrict__ ptr, const int* __restric
     const int p = ptr[c];
     if (c == 0 && p != 0) b |= 1;
     if (c == n && p != nnz) b |= 2;
-    if (c < n && ptr[c + 1] < p) b |= 4;
-  }
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += stride) {
-    const int r = idx[e];
-    if (r < 0 || r >= n) b |= 8;
+    if (c < n) {
+      const int q = ptr[c + 1];
+      if (q < p) {
+        b |= 4;
+      } else if (p >= 0 && q <= nnz) {
+        int prev = -1;
+        for (int e = p; e < q; ++e) {
+          const int r = __ldg(idx + e);
+          if (r < 0 || r >= n) b |= 8;
+          if (e > p) b |= r == prev ? 32 : (r < prev ? 16 : 0);
+          prev = r;
+        }
+      }
+    }
   }
   if (b) atomicOr(bad, b);
+}
+
+// Duplicate rows inside unsorted columns (run only when k_validate_csc found
+// one, after it passed): one warp per column compares every pair of entries,
+// 32 x 32 per step through shuffles, so a column of L entries costs L^2 / 32
+// comparisons per lane.  Sorted columns are skipped by a neighbour check.
+__global__ void k_csc_duplicates(const int* __restrict__ ptr, const int* __restrict__ idx, int n,
+                                 int* __restrict__ bad) {
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < n; c += warps) {
+    const int p = ptr[c], len = ptr[c + 1] - p;
+    if (len < 2) continue;
+    bool desc = false;
+    for (int e = lane + 1; e < len; e += 32) desc |= idx[p + e] < idx[p + e - 1];
+    if (!__any_sync(0xffffffffu, desc)) continue;
+    bool dup = false;
+    for (int a = 0; a < len; a += 32) {
+      const int v = a + lane < len ? idx[p + a + lane] : -1;
+      for (int bb = a; bb < len; bb += 32) {
+        const int w = bb + lane < len ? idx[p + bb + lane] : -2;
+        const int lim = min(32, len - bb);
+        for (int s = 0; s < lim; ++s) {
+          const int ws = __shfl_sync(0xffffffffu, w, s);
+          dup |= v >= 0 && (bb > a || s > lane) && v == ws;
+        }
+      }
+    }
+    if (__any_sync(0xffffffffu, dup) && lane == 0) atomicOr(bad, 32);
+  }
 }
 
 __global__ void k_iota(int* __restrict__ out, int n) {
@@ -398,21 +443,31 @@ int sampled_outer(Ctx* c, int n, const int* ptr, const int* idx, const double* u
   return DCU_OK;
 }
 
-int validate_csc(Ctx* c, int n, int nnz, const int* ptr, const int* idx) {
+int validate_csc(Ctx* c, int n, int nnz, const int* ptr, const int* idx, bool unique_rows) {
   DCU_TRY(ensure(c, B_ROWCNT, sizeof(int) * (size_t)(n + 1)));
   int* bad = bp<int>(c, B_ROWCNT);
   DCU_CUDA(c, cudaMemsetAsync(bad, 0, sizeof(int), c->stream));
-  k_validate_csc<<<waves_grid(c, (long long)(nnz > n ? nnz : n + 1), 256, 8), 256, 0, c->stream>>>(ptr, idx, n, nnz,
-                                                                                                   bad);
+  k_validate_csc<<<waves_grid(c, (long long)n + 1, 256, 8), 256, 0, c->stream>>>(ptr, idx, n, nnz, bad);
   DCU_LAUNCHED(c, "k_validate_csc");
   DCU_CUDA(c, cudaMemcpyAsync(c->pinned, bad, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   DCU_CUDA(c, cudaStreamSynchronize(c->stream));
-  const int b = *(int*)c->pinned;
-  if (b) {
+  int b = *(int*)c->pinned;
+  if (b & 15) {
     return fail(c, DCU_ERR_ARG, "malformed CSC matrix:%s%s%s%s", (b & 1) ? " ptr[0] != 0;" : "",
                 (b & 2) ? " ptr[n] != nnz;" : "", (b & 4) ? " ptr decreases;" : "",
                 (b & 8) ? " row index out of [0, n);" : "");
   }
+  if (!unique_rows) return DCU_OK;
+  if ((b & 16) && !(b & 32)) {
+    k_csc_duplicates<<<waves_grid(c, (long long)n * 32, 256, 8), 256, 0, c->stream>>>(ptr, idx, n, bad);
+    DCU_LAUNCHED(c, "k_csc_duplicates");
+    DCU_CUDA(c, cudaMemcpyAsync(c->pinned, bad, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    DCU_CUDA(c, cudaStreamSynchronize(c->stream));
+    b = *(int*)c->pinned;
+  }
+  if (b & 32)
+    return fail(c, DCU_ERR_ARG, "malformed CSC matrix: a column holds the same row index twice (duplicate entries "
+                                "are not accepted; sum them first)");
   return DCU_OK;
 }
 

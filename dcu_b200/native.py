@@ -11,6 +11,7 @@ import os
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "lib", "libdcu_spai.so")
 CLI_PATH = os.path.join(_HERE, "lib", "spai_multi_dcu")
+CLI_SINGLE_PATH = os.path.join(_HERE, "lib", "spai_single_dcu")
 
 # dcu_status
 OK, ERR_ARG, ERR_CUDA, ERR_ALLOC, ERR_NO_DEVICE, ERR_LIMIT = range(6)

@@ -26,7 +26,13 @@
  * Matrices are square, CSC, 0-based: ptr[n+1] (int32), idx[nnz] row indices
  * (int32), val[nnz] (float64) -- the CSC_Matrix layout of
  * include/common/dataType.h:33-41.  The preconditioner M has A's pattern, so
- * it is passed as values only (mval[nnz], aligned with A's idx).
+ * it is passed as values only (mval[nnz], aligned with A's idx).  A row index
+ * may appear only once per column: the SPAI and solver entry points refuse a
+ * repeated (row, column) pair with DCU_ERR_ARG.  (The reference's gather
+ * takes the first match, src/spai_multi_dcu.cpp:945-983, and its J_k then
+ * holds the column twice: two equal columns of A(I,J), a zero R pivot and a
+ * NaN column of M.)  dcu_csc_to_csr_d and dcu_sampled_outer_d accept
+ * repeated pairs.  Columns may list their rows in any order.
  * Suffix _d: device pointers (cudaMalloc'ed, on the context's device; the
  * solution vector x must be 16-byte aligned, as cudaMalloc and torch
  * allocations are, else DCU_ERR_ARG);
