@@ -92,3 +92,48 @@ def test_non_finite_values_end_in_breakdown(ctx):
     b, _ = W.rhs_from_solution(A, seed=1)
     x, _, _, si = ctx.solve_h(A, b)
     assert si.status == N.SOLVE_CONVERGED and np.linalg.norm(b - A.matvec(x)) / np.linalg.norm(b) < 1e-8
+
+
+def _duplicated():
+    """Matrices whose column holds one row index twice: adjacent in a sorted
+    column, apart in an unsorted one, and 40 places apart in a long unsorted
+    column (past one warp's 32 entries)."""
+    from tests.test_gpu_pattern import random_csc
+
+    out = {}
+    A = W.convdiff2d(8, 1.0)
+    p = int(A.ptr[10])
+    i = A.idx.copy()
+    i[p + 1] = i[p]
+    out["sorted_adjacent"] = (A, i)
+    i = A.idx.copy()
+    r0, r1, r2 = (int(v) for v in A.idx[p:p + 3])
+    i[p:p + 3] = [r1, r2, r1]
+    out["unsorted_apart"] = (A, i)
+    B = random_csc(300, 0.3, 5)                 # ~90 entries per column, shuffled
+    c = int(np.argmax(np.diff(B.ptr)))
+    q = int(B.ptr[c])
+    i = B.idx.copy()
+    i[q + 45] = i[q + 5]
+    out["long_unsorted"] = (B, i)
+    return out
+
+
+@pytest.mark.parametrize("case", ["sorted_adjacent", "unsorted_apart", "long_unsorted"])
+def test_duplicate_rows_are_refused(ctx, case):
+    import torch
+
+    A, idx = _duplicated()[case]
+    rc = _build_raw(ctx, A.n, A.nnz, A.ptr.astype(np.int32), idx.astype(np.int32), A.val.copy())
+    assert rc == N.ERR_ARG, rc
+    assert b"same row index twice" in ctx._L.dcu_spai_last_error(ctx.h)
+    # the format conversion accepts the pair, as the reference's does
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    rp = torch.zeros(A.n + 1, dtype=torch.int32, device="cuda")
+    ri = torch.zeros(A.nnz, dtype=torch.int32, device="cuda")
+    rv = torch.zeros(A.nnz, dtype=torch.float64, device="cuda")
+    ctx.csc_to_csr_d(A.n, A.nnz, d(A.ptr), d(idx.astype(np.int32)), d(A.val), rp, ri, rv)
+    assert int(rp[-1].item()) == A.nnz
+    # and the same matrix without the repeat, in shuffled order, builds
+    m, _, info = ctx.build_h(A)
+    assert info.cols_total == A.n and np.isfinite(m).all()
