@@ -164,6 +164,10 @@ class Context:
         self._check(self._L.dcu_sell_plan_stats(self.h, C.byref(s), C.byref(u), C.byref(w)))
         return (s.value, u.value, w.value) if wide else (s.value, u.value)
 
+    def set_wide_prepass(self, enabled: bool):
+        """Wide-slice pre-pass of later solves on (default) or off (dcu_set_wide_prepass)."""
+        self._check(self._L.dcu_set_wide_prepass(self.h, 1 if enabled else 0))
+
     def autotune_d(self, n, nnz, ptr_d, idx_d, val_d, b_d, reps: int = 10, **opt) -> "N.Tuning":
         """Time the launch configurations of opt's precision form on this matrix and keep the fastest
         for later builds and solves of that form on this context (dcu_autotune_d)."""

@@ -709,6 +709,12 @@ int dcu_sell_plan_stats(dcu_spai_ctx* c, long long* slots, long long* uniform_sl
   return dcu::plan_stats(c, slots, uniform_slots, wide_slices);
 }
 
+int dcu_set_wide_prepass(dcu_spai_ctx* c, int enabled) {
+  if (!c) return DCU_ERR_ARG;
+  c->wide_prepass = enabled != 0;
+  return DCU_OK;
+}
+
 int dcu_profile_iteration_kernels(dcu_spai_ctx* c, int reps, float* ms_out, int cap, int* count) {
   if (!c || !ms_out) return DCU_ERR_ARG;
   StreamScope scope(c);

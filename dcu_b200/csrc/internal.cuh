@@ -112,6 +112,7 @@ struct Ctx {
   bool profile_k1_free = false;    // fused and split first steps compute the same values
   int profile_default_split = 0;   // the form's default first step
   int plan_wide = 0;               // slices of the last SELL plan wider than kWideSlice
+  bool wide_prepass = true;        // flag wide slices for the pre-pass (dcu_set_wide_prepass)
 };
 
 // Iteration kernels of BiCGSTAB, for profiling and the autotuner.

@@ -11,7 +11,6 @@
 //          256 bytes for FP64).  Padding slots carry column = r and perm = -1.
 //          del int16 holds col - r when every |col - r| < 32768.
 #include <climits>
-#include <mutex>
 
 #include "internal.cuh"
 
@@ -293,7 +292,7 @@ __global__ void k_sell_delta(const int* __restrict__ sidx, long long slots, int 
 // every k of the slice has one offset (the SpMV then reads no index at all).
 __global__ void k_sell_desc(const int* __restrict__ sidx, int n, int nslices, const long long* __restrict__ off,
                             int* __restrict__ kd, int* __restrict__ su, unsigned long long* __restrict__ uslots,
-                            const int* __restrict__ rptr, int* __restrict__ wide) {
+                            const int* __restrict__ rptr, int* __restrict__ wide, int allow_wide) {
   const int rows_total = nslices * 32;
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows_total; r += gridDim.x * blockDim.x) {
     const int s = r >> 5, lane = r & 31;
@@ -314,7 +313,7 @@ __global__ void k_sell_desc(const int* __restrict__ sidx, int n, int nslices, co
       int f = all ? 1 : 0;
       // a full slice made wide by a few long rows: listed for the solver's
       // pre-pass (wide[0] counts, wide[1 + i] = slice)
-      if (w > kWideSlice && nlong <= kWideRows && 32 * s + 32 <= n) {
+      if (allow_wide && w > kWideSlice && nlong <= kWideRows && 32 * s + 32 <= n) {
         const int i = atomicAdd(wide, 1);
         wide[1 + i] = s;
         f |= 4 | (i << 3);
@@ -574,7 +573,8 @@ int sell_fill_from_csr(Ctx* c, int n, int nnz, const int* rptr, const int* rcol,
   int* wide = bp<int>(c, B_SELL_WIDE);
   DCU_CUDA(c, cudaMemsetAsync(wide, 0, sizeof(int), c->stream));
   k_sell_desc<<<waves_grid(c, (long long)nslices * 32, 256, 8), 256, 0, c->stream>>>(sidx, n, nslices, off, kd, su,
-                                                                                       pst + 1, rptr, wide);
+                                                                                       pst + 1, rptr, wide,
+                                                                                       c->wide_prepass ? 1 : 0);
   DCU_LAUNCHED(c, "k_sell_desc");
   DCU_CUDA(c, cudaMemcpyAsync(c->pinned, wide, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   DCU_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -715,27 +715,13 @@ __global__ void __launch_bounds__(512) k_row_sort_long_smem(const int* __restric
   }
 }
 
-// Device address of g_noalloc_scratch, looked up once per device (with that
-// device current) on the first call there.
-void* noalloc_scratch_for_device(int device, cudaError_t* err) {
-  static std::mutex mu;
-  static void* addr[64] = {nullptr};
-  *err = cudaSuccess;
-  if (device < 0 || device >= 64) {
-    *err = cudaErrorInvalidDevice;
-    return nullptr;
-  }
-  std::lock_guard<std::mutex> lock(mu);
-  if (!addr[device]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) {
-      *err = e;
-      return nullptr;
-    }
-    addr[device] = p;
-  }
-  return addr[device];
+// Device address of g_noalloc_scratch on the current device, looked up on
+// every call: the lookup is a host-side table read, and a cached address
+// would go stale if the device's context were reset and the module reloaded.
+void* noalloc_scratch_address(cudaError_t* err) {
+  void* p = nullptr;
+  *err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  return *err == cudaSuccess ? p : nullptr;
 }
 
 }  // namespace
@@ -747,11 +733,20 @@ extern "C" int dcu_csc_to_csr_noalloc_d(int n, int nnz, const int* ptr, const in
   if (n <= 0 || nnz < 0 || !ptr || !rptr || (nnz > 0 && (!idx || !ridx))) return DCU_ERR_ARG;
   if (n > kNoAllocMaxN || nnz > kNoAllocMaxNnz) return DCU_ERR_LIMIT;
   cudaStream_t st = (cudaStream_t)stream_ptr;
-  int device = 0;
-  if (cudaGetDevice(&device) != cudaSuccess) return DCU_ERR_CUDA;
+  // The call synchronises the stream and reads flags back to the host, which
+  // a stream under capture does not allow: refuse it before touching it.
+  cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &capture) != cudaSuccess) {
+    cudaGetLastError();
+    return DCU_ERR_ARG;
+  }
+  if (capture != cudaStreamCaptureStatusNone) return DCU_ERR_ARG;
   cudaError_t e = cudaSuccess;
-  char* base = static_cast<char*>(noalloc_scratch_for_device(device, &e));
-  if (!base) return e == cudaErrorInvalidDevice ? DCU_ERR_NO_DEVICE : DCU_ERR_CUDA;
+  char* base = static_cast<char*>(noalloc_scratch_address(&e));
+  if (!base) {
+    cudaGetLastError();
+    return e == cudaErrorNoDevice || e == cudaErrorInvalidDevice ? DCU_ERR_NO_DEVICE : DCU_ERR_CUDA;
+  }
   int* cnt = reinterpret_cast<int*>(base + kNoAllocCnt);
   int* longrows = reinterpret_cast<int*>(base + kNoAllocLong);
   int* longcount = longrows + n;  // [0] count, [1] longest
@@ -775,7 +770,9 @@ extern "C" int dcu_csc_to_csr_noalloc_d(int n, int nnz, const int* ptr, const in
   NOALLOC_CHECK(cudaGetLastError());
   NOALLOC_CHECK(cudaMemcpyAsync(host_flags, flags, sizeof(int), cudaMemcpyDeviceToHost, st));
   NOALLOC_CHECK(cudaStreamSynchronize(st));
-  if (host_flags[0]) return DCU_ERR_ARG;
+  // bits 1-8: malformed ptr / idx; the conversion accepts unsorted columns
+  // and repeated rows (bits 16 and 32 of the shared check)
+  if (host_flags[0] & 15) return DCU_ERR_ARG;
   if (nnz > 0) {
     k_row_count<<<grid_z, 256, 0, st>>>(idx, nnz, cnt);
     NOALLOC_CHECK(cudaGetLastError());

@@ -90,6 +90,7 @@ SIGNATURES = {
                                C.POINTER(BuildInfo), C.POINTER(SolveInfo)]),
     "dcu_profile_iteration_kernels": (_i, [_vp, _i, C.POINTER(C.c_float), _i, C.POINTER(_i)]),
     "dcu_sell_plan_stats": (_i, [_vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
+    "dcu_set_wide_prepass": (_i, [_vp, _i]),
     "dcu_tuning_default": (None, [C.POINTER(Tuning)]),
     "dcu_set_tuning": (_i, [_vp, _i, C.POINTER(Tuning)]),
     "dcu_get_tuning": (_i, [_vp, _i, C.POINTER(Tuning)]),

@@ -207,10 +207,14 @@ int dcu_csc_to_csr_d(dcu_spai_ctx* ctx, int n, int nnz, const int* ptr, const in
  * process exits.  Limits: n <= 131072, nnz <= 1048576 (DCU_ERR_LIMIT beyond),
  * no row longer than 8192 entries (DCU_ERR_LIMIT after the call).  Runs on
  * `stream` (a cudaStream_t, NULL = legacy default) on the current device and
- * returns after it finished there.  The first call on a device looks up the
- * array's device address there; make that first call before any stream
- * capture.  Every call reuses the same array (the parts that must start at
- * zero are cleared each time), so calls that overlap on one GPU race.
+ * returns after it finished there: it synchronises the stream and reads a
+ * status back to the host, and returns DCU_ERR_ARG without using a stream
+ * that is capturing.  Each call looks up the array's device address on the
+ * current device.  Every call reuses the same array (the parts that must
+ * start at zero are cleared each time), so calls that overlap on one GPU
+ * race.  After a return other than DCU_OK the outputs are undefined (they may
+ * be partly written).  Duplicate (row, column) pairs and unsorted columns are
+ * accepted, as by dcu_csc_to_csr_d.
  * No counterpart in the reference. */
 int dcu_csc_to_csr_noalloc_d(int n, int nnz, const int* ptr, const int* idx, const double* val,
                              int* rptr, int* ridx, double* rval, void* stream);
@@ -293,6 +297,13 @@ int dcu_profile_iteration_kernels(dcu_spai_ctx* ctx, int reps, float* ms_out, in
  * warp-cooperative pre-pass sums before each SpMV.  Any output may be NULL.  No counterpart in the
  * reference. */
 int dcu_sell_plan_stats(dcu_spai_ctx* ctx, long long* slots, long long* uniform_slots, long long* wide_slices);
+
+/* Turn the wide-slice pre-pass of this context's later solves on (enabled !=
+ * 0, the default) or off (every slice's rows summed by the SpMV kernels'
+ * per-lane loop).  Each row is summed in its own order either way, so the
+ * two give bit-identical iterates; off exists to show that, and to time the
+ * pre-pass.  No counterpart in the reference. */
+int dcu_set_wide_prepass(dcu_spai_ctx* ctx, int enabled);
 
 /* ---- autotuner (no counterpart in the reference) ----------------------------- */
 

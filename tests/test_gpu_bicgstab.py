@@ -179,3 +179,33 @@ def test_sell_plan_stats_and_offset_aligned_slices(ctx):
         ref = oracle.bicgstab(A, m_o, b, None, tol=1e-8, tol_mode="rel", maxiter=1000)
         assert si.status == N.SOLVE_CONVERGED and abs(si.iters - ref["iters"]) <= 1
         assert np.linalg.norm(b - A.matvec(x)) / np.linalg.norm(b) < 1e-8
+
+
+@pytest.mark.parametrize("prec", [N.PREC_FP64, N.PREC_M_BF16])
+def test_wide_prepass_keeps_iterates_bit_identical(ctx, prec):
+    """The circuit-like matrix's hub rows make wide SELL slices, summed by the
+    warp-cooperative pre-pass (each row in its own order, long rows by one
+    chain in k order).  With the pre-pass off the SpMV kernels' per-lane loop
+    sums the same rows: the iterates and the count must not change by a bit."""
+    import torch
+
+    A = W.circuit_like()
+    rng = np.random.Generator(np.random.PCG64(11))
+    b = rng.uniform(-1, 1, A.n)
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    ptr, idx, val, bd = d(A.ptr), d(A.idx), d(A.val), d(b)
+    out = []
+    try:
+        for on in (True, False):
+            ctx.set_wide_prepass(on)
+            x = torch.zeros(A.n, dtype=torch.float64, device="cuda")
+            bi, si = ctx.solve_d(A.n, A.nnz, ptr, idx, val, bd, x, precision=prec)
+            _, _, nwide = ctx.sell_plan_stats(wide=True)
+            assert (nwide > 0) == on
+            assert si.status == N.SOLVE_CONVERGED
+            out.append((x.cpu().numpy(), si.iters, si.res))
+    finally:
+        ctx.set_wide_prepass(True)
+    assert out[0][1] == out[1][1]
+    assert np.array_equal(out[0][0], out[1][0])
+    assert out[0][2] == out[1][2]
