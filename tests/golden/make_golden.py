@@ -107,12 +107,39 @@ def _perturbed(m, seed):
     return np.where(s, np.nextafter(m, np.inf), np.nextafter(m, -np.inf))
 
 
+def _block(A, s0, s1):
+    sub_ptr = A.ptr[s0:s1 + 1] - A.ptr[s0]
+    return W.CSC(s1 - s0, sub_ptr.astype(np.int32), (A.idx[A.ptr[s0]:A.ptr[s1]] - s0).astype(np.int32),
+                 A.val[A.ptr[s0]:A.ptr[s1]])
+
+
+def batch_sensitivity(trials=4, systems=64):
+    """The same spread for every (system, right-hand side) pair of the first
+    `systems` systems of the 512-system batch: the largest over the pairs."""
+    bt = W.batch_systems()
+    off = bt.offsets[: systems + 1].astype(np.int64)
+    worst, moved = 0, 0
+    for s in range(systems):
+        As = _block(bt.A, int(off[s]), int(off[s + 1]))
+        m, _, _, _ = oracle.spai(As, "mgs")
+        mps = [_perturbed(m, t) for t in range(1, trials + 1)]
+        for q in range(bt.B.shape[1]):
+            b = bt.B[off[s]:off[s + 1], q]
+            base = oracle.bicgstab(As, m, b, None, tol=1e-8, tol_mode="rel", maxiter=1000)["iters"]
+            d = max(abs(oracle.bicgstab(As, mp, b, None, tol=1e-8, tol_mode="rel", maxiter=1000)["iters"] - base)
+                    for mp in mps)
+            worst = max(worst, d)
+            moved += d > 0
+    return {"iters_band": max(1, worst), "pairs": systems * bt.B.shape[1], "pairs_moved": moved,
+            "trials": trials}
+
+
 def sensitivity(trials=8):
     """Spread of the oracle's own BiCGSTAB iteration count when M moves by one
     ulp per value, on the benchmark workloads with long solves: the band a
     solver with another summation order can be held to.  Writes
     tests/golden/sensitivity.json."""
-    out = {}
+    out = {"batch512_first64": batch_sensitivity()}
     A = W.varcoef2d(512, seed=5)
     rng = np.random.Generator(np.random.PCG64(5))
     b, xt = rng.standard_normal(A.n), rng.standard_normal(A.n)
@@ -149,5 +176,11 @@ def sensitivity(trials=8):
 if __name__ == "__main__":
     if "--sensitivity" in sys.argv:
         sensitivity()
+    elif "--batch-sensitivity" in sys.argv:
+        path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "sensitivity.json")
+        out = json.load(open(path))
+        out["batch512_first64"] = batch_sensitivity()
+        with open(path, "w") as f:
+            json.dump(out, f, indent=1, sort_keys=True)
     else:
         main()

@@ -148,9 +148,17 @@ def _block(A, s0, s1):
 
 def test_batch512_first_64_systems(ctx):
     """The first 64 systems of the 512-system batch, exactly as generated for
-    the benchmark (same seed and size distribution), solved as one batch."""
+    the benchmark (same seed and size distribution), solved as one batch.
+    Every pair's count within the spread the oracle itself shows when M moves
+    by one ulp (tests/golden/sensitivity.json: 44 of the 512 pairs move, by
+    up to 3 iterations)."""
+    import json
+    import os
+
     import torch
 
+    band = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "sensitivity.json")))[
+        "batch512_first64"]["iters_band"]
     bt = W.batch_systems()
     ns = 64
     off = bt.offsets[: ns + 1].astype(np.int64)
@@ -175,4 +183,4 @@ def test_batch512_first_64_systems(ctx):
             x = Xh[s0:s1, q]
             assert np.linalg.norm(b - As.matvec(x)) / np.linalg.norm(b) < 1e-8
             worst = max(worst, abs(int(iters[s, q]) - ref["iters"]))
-    assert worst <= 1, worst
+    assert worst <= band, (worst, band)

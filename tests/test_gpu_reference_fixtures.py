@@ -9,9 +9,15 @@ row), blocks far beyond one CTA's shared memory.  Expected values are the
 oracle's (tests/golden/golden.json, "fixtures"): M within 1e-10 of the
 Householder oracle (which matches the MGS oracle to 5e-13 on every column),
 BiCGSTAB iterations within one of the oracle's in the reference's solver
-settings and in the configs'.  fill_3elt does not converge in either setting
-(the oracle runs to MAX_ITER with a finite residual): the GPU must do the
-same, ending with the maxiter status and the reference's counter."""
+settings and in the configs'.  fill_3elt does not converge in either setting.
+Its iterates wander without converging, and whether a recurrence scalar
+(rho, (r*, A y)) comes out exactly zero on the way depends on the summation
+order: the oracle and the reference's own BiCGSTAB code over the stand-in
+sums reach MAX_ITER with a finite residual, a numpy restatement meets rho = 0
+at iteration 1656.  Where that happens the reference's code carries NaN on to
+MAX_ITER; here the solver stops with the breakdown status.  So the GPU must end
+unconverged with either status, and the reference-compatible count (the
+legacy entry point, through the driver) is MAX_ITER either way."""
 import hashlib
 import os
 import re
@@ -94,15 +100,32 @@ def test_fill3elt_runs_to_maxiter(ctx):
     assert info.cols_singular == g["singular"]
     assert np.max(np.abs(m - m_o)) <= 1e-10 * np.max(np.abs(m_o))
     rs = g["reference_settings"]
+    assert rs["status"] == N.SOLVE_MAXITER and rs["iters"] == 10000
     x, si = ctx.bicgstab_h(A, m, np.ones(A.n), np.ones(A.n), tol=1e-7, tol_mode=N.TOL_ABS, maxiter=10000,
                            verify=0)
-    assert rs["status"] == N.SOLVE_MAXITER and si.status == N.SOLVE_MAXITER
-    assert si.iters == rs["iters"] == 10000     # the counter ends at MAX_ITER
-    assert np.isfinite(si.res)
+    info = (si.status, si.iters, si.res)
+    assert si.status in (N.SOLVE_MAXITER, N.SOLVE_BREAKDOWN), info
+    if si.status == N.SOLVE_MAXITER:
+        assert si.iters == 10000 and np.isfinite(si.res), info   # the counter ends at MAX_ITER
+    else:
+        assert si.iters < 10000 and si.res >= 1e-7, info
     cs = g["config_settings"]
+    assert cs["status"] == N.SOLVE_MAXITER and cs["iters"] == 1000
     b = W.rhs_ones_product(A)
     x, _, bi, si = ctx.solve_h(A, b)
-    assert cs["status"] == N.SOLVE_MAXITER and si.status == N.SOLVE_MAXITER and si.iters == 1000
+    info = (si.status, si.iters, si.res)
+    assert si.status in (N.SOLVE_MAXITER, N.SOLVE_BREAKDOWN), info
+    assert si.status == N.SOLVE_BREAKDOWN or si.iters == 1000, info
+
+
+def test_fill3elt_driver_reports_max_iter():
+    """The legacy entry point (runBiCGSTABOnRank0, through spai_multi_dcu)
+    returns the reference's count on a non-converging system: MAX_ITER."""
+    path, A, g = _load("fill_3elt.mtx")
+    out = subprocess.run([N.CLI_PATH, "--matrix", path], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    m = re.search(r"iteration_count=(\d+)$", out.stdout, re.M)
+    assert m and int(m.group(1)) == 10000, out.stdout
 
 
 def _ref_dir():
