@@ -60,23 +60,87 @@ __device__ __forceinline__ int ldcol(const int16_t* ix, long long q, int r) { re
 template <typename T>
 __device__ __forceinline__ double ldv(const T* p) { return (double)__ldg(p); }
 
+// kNarrow values of one row of a narrow slice, read row-major from the
+// narrow array (an FP32 / BF16 M): one 16-byte load for BF16, two for FP32.
+template <typename MT>
+struct Row8;
+template <>
+struct Row8<__nv_bfloat16> {
+  uint4 u;
+  __device__ __forceinline__ void load(const __nv_bfloat16* p) { u = __ldcs(reinterpret_cast<const uint4*>(p)); }
+  __device__ __forceinline__ double at(int t) const {
+    const unsigned w = (t < 2) ? u.x : (t < 4) ? u.y : (t < 6) ? u.z : u.w;
+    return (double)__uint_as_float((t & 1) ? (w & 0xffff0000u) : (w << 16));
+  }
+};
+template <>
+struct Row8<float> {
+  float4 a, b;
+  __device__ __forceinline__ void load(const float* p) {
+    a = __ldcs(reinterpret_cast<const float4*>(p));
+    b = __ldcs(reinterpret_cast<const float4*>(p) + 1);
+  }
+  __device__ __forceinline__ double at(int t) const {
+    const float4& q = (t < 4) ? a : b;
+    const int u = t & 3;
+    return (double)((u == 0) ? q.x : (u == 1) ? q.y : (u == 2) ? q.z : q.w);
+  }
+};
+template <>
+struct Row8<double> {  // never loaded: an FP64 M has no narrow array
+  __device__ __forceinline__ void load(const double*) {}
+  __device__ __forceinline__ double at(int) const { return 0.0; }
+};
+
 // One SELL-32 row: sum_k val[q] * xf(col[q]).  A warp covers one slice, so
 // each k step reads 32 consecutive slots.  Slots are taken 8 at a time with
 // every value and index load issued before the dependent gathers, so a thread
 // keeps up to 16 independent loads in flight.  A slice whose every k has one
 // column offset for all its rows (su[s]; SellPlan::kd) reads no index at all:
 // the column is the row plus the slice's offset, one broadcast load per k
-// from a table 1/32 the size of the index array.  The rows of a slice that
-// the plan flagged wide (su bit 2) were summed by the wide pre-pass
-// (k_bi_wide) into wv.
-template <typename MT, typename IT, typename F>
+// from a table 1/32 the size of the index array.  For a narrow slice (at most
+// kNarrow wide, SellPlan::kd8) those offsets come from a table indexed by the
+// slice, so they load together with the slice's flags and slot offset rather
+// than after them; with M8 (an FP32 / BF16 M) its values come row-major from
+// val8 as well, so a row needs one round trip for its values and offsets and
+// one for its gathers.  Every path sums the row's products in entry order.
+// The rows of a slice that the plan flagged wide (su bit 2) were summed by
+// the wide pre-pass (k_bi_wide) into wv.
+template <bool M8, typename MT, typename IT, typename F>
 __device__ __forceinline__ double sell_row(const long long* __restrict__ off, const int* __restrict__ kd,
-                                           const int* __restrict__ su, const double* __restrict__ wv,
-                                           const MT* __restrict__ val, const IT* __restrict__ ix, int r, F xf) {
+                                           const int* __restrict__ kd8, const int* __restrict__ su,
+                                           const double* __restrict__ wv, const MT* __restrict__ val,
+                                           const MT* __restrict__ val8, const IT* __restrict__ ix, int r, F xf) {
   const int s = r >> 5;
   const int f = __ldg(su + s);
+  const int4* kq = reinterpret_cast<const int4*>(kd8 + (long long)s * kNarrow);
+  const int4 da = __ldg(kq), db = __ldg(kq + 1);
+  Row8<MT> m8;
+  long long o0 = 0, o1 = 0;
+  if (M8) {
+    m8.load(val8 + (long long)r * kNarrow);
+  } else {
+    o0 = __ldg(off + s);
+    o1 = __ldg(off + s + 1);
+  }
   if (f & 4) return __ldg(wv + ((long long)(f >> 3) << 5) + (r & 31));
-  const long long o0 = __ldg(off + s), o1 = __ldg(off + s + 1);
+  if (f & 2) {
+    const int w = (f >> 3) & 15;
+    const int d[kNarrow] = {da.x, da.y, da.z, da.w, db.x, db.y, db.z, db.w};
+    double av[kNarrow];
+    const long long base = o0 + (r & 31);
+#pragma unroll
+    for (int t = 0; t < kNarrow; ++t) av[t] = (t < w) ? (M8 ? m8.at(t) : ldm(val + base + 32ll * t)) : 0.0;
+    double acc = 0.0;
+#pragma unroll
+    for (int t = 0; t < kNarrow; ++t)
+      if (t < w) acc += av[t] * xf(r + d[t]);
+    return acc;
+  }
+  if (M8) {
+    o0 = __ldg(off + s);
+    o1 = __ldg(off + s + 1);
+  }
   const long long base = o0 + (r & 31);
   const int w = (int)((o1 - o0) >> 5);
   double acc = 0.0;
@@ -176,10 +240,12 @@ struct BiArgs {
   int n;
   const long long* off;
   const int* kd;        // per (slice, k) offset descriptors (SellPlan::kd)
-  const int* su;        // per slice: all of its k uniform (SellPlan::su)
+  const int* kd8;       // per narrow slice, its offsets (SellPlan::kd8)
+  const int* su;        // per slice flags (SellPlan::su)
   const IT* ix;         // shared by A and M (same pattern)
   const double* aval;
   const MT* mval;
+  const MT* mval8;      // narrow slices' M values, row-major (FP32 / BF16 M), or null
   const double* b;
   double* x;
   double* r;
@@ -198,6 +264,19 @@ struct BiArgs {
   double* wide_val;      // their row values for the next SpMV, 32 per listed slice
   int nwide;
 };
+
+// A's row (FP64 values in SELL order).
+template <typename MT, typename IT, typename VT, typename F>
+__device__ __forceinline__ double a_row(const BiArgs<MT, IT, VT>& a, int r, F xf) {
+  return sell_row<false, double, IT>(a.off, a.kd, a.kd8, a.su, a.wide_val, a.aval, nullptr, a.ix, r, xf);
+}
+// M's row: narrow slices from the row-major narrow array where the form has one.
+template <typename MT, typename IT, typename VT, typename F>
+__device__ __forceinline__ double m_row(const BiArgs<MT, IT, VT>& a, int r, F xf) {
+  constexpr bool narrow = !std::is_same<MT, double>::value;
+  if (narrow && a.mval8) return sell_row<narrow, MT, IT>(a.off, a.kd, a.kd8, a.su, a.wide_val, a.mval, a.mval8, a.ix, r, xf);
+  return sell_row<false, MT, IT>(a.off, a.kd, a.kd8, a.su, a.wide_val, a.mval, nullptr, a.ix, r, xf);
+}
 
 // Kernels K1..K5 are launched with programmatic dependent launch: their blocks
 // may start while the previous kernel drains, and wait here for its results.
@@ -331,7 +410,7 @@ __global__ void __launch_bounds__(BI_BLOCK) k_bi_init(BiArgs<MT, IT, VT> a, doub
   double v[3] = {0.0, 0.0, 0.0};
   const int stride = gridDim.x * BI_BLOCK;
   for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) {
-    const double ax = sell_row(a.off, a.kd, a.su, a.wide_val, a.aval, a.ix, r, [&](int c) { return ldv(a.x + c); });
+    const double ax = a_row(a, r, [&](int c) { return ldv(a.x + c); });
     const double br = a.b[r];
     const double rr = br + (-1.0) * ax;
     a.r[r] = rr;
@@ -386,7 +465,7 @@ __global__ void __launch_bounds__(BI_BLOCK) k_bi_py(BiArgs<MT, IT, VT> a) {
   auto pf = [&](int c) { return ldv(rr + c) + beta * (ldv(pold + c) - omega * ldv(ay + c)); };
   const int stride = gridDim.x * BI_BLOCK;
   for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) {
-    const double yv = sell_row(a.off, a.kd, a.su, a.wide_val, a.mval, a.ix, r, pf);
+    const double yv = m_row(a, r, pf);
     pnew[r] = (VT)pf(r);
     a.y[r] = (VT)yv;
   }
@@ -444,7 +523,7 @@ __global__ void __launch_bounds__(BI_BLOCK, 8) k_bi_y(BiArgs<MT, IT, VT> a) {
   const VT* __restrict__ p = a.p0;
   const int stride = gridDim.x * BI_BLOCK;
   for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride)
-    a.y[r] = (VT)sell_row(a.off, a.kd, a.su, a.wide_val, a.mval, a.ix, r, [&](int c) { return ldv(p + c); });
+    a.y[r] = (VT)m_row(a, r, [&](int c) { return ldv(p + c); });
 }
 
 // K2: ay = A y; alpha = rho / (r*, ay)
@@ -459,7 +538,7 @@ __global__ void __launch_bounds__(BI_BLOCK, (std::is_same<MT, double>::value || 
   const VT* __restrict__ y = a.y;
   const int stride = gridDim.x * BI_BLOCK;
   for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) {
-    const double ayv = sell_row(a.off, a.kd, a.su, a.wide_val, a.aval, a.ix, r, [&](int c) { return ldv(y + c); });
+    const double ayv = a_row(a, r, [&](int c) { return ldv(y + c); });
     a.ay[r] = ayv;
     v[0] += (double)a.rs[r] * ayv;
   }
@@ -485,7 +564,7 @@ __global__ void __launch_bounds__(BI_BLOCK) k_bi_sz(BiArgs<MT, IT, VT> a) {
   auto sf = [&](int c) { return ldv(rr + c) + nalpha * ldv(ay + c); };
   const int stride = gridDim.x * BI_BLOCK;
   for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) {
-    const double zv = sell_row(a.off, a.kd, a.su, a.wide_val, a.mval, a.ix, r, sf);
+    const double zv = m_row(a, r, sf);
     a.s[r] = rr[r] + nalpha * ay[r];
     a.z[r] = (VT)zv;
   }
@@ -499,7 +578,7 @@ __global__ void __launch_bounds__(BI_BLOCK) k_bi_az(BiArgs<MT, IT, VT> a) {
   const VT* __restrict__ z = a.z;
   const int stride = gridDim.x * BI_BLOCK;
   for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) {
-    const double azv = sell_row(a.off, a.kd, a.su, a.wide_val, a.aval, a.ix, r, [&](int c) { return ldv(z + c); });
+    const double azv = a_row(a, r, [&](int c) { return ldv(z + c); });
     a.az[r] = azv;
     v[0] += azv * a.s[r];
     v[1] += azv * azv;
@@ -594,7 +673,7 @@ __global__ void __launch_bounds__(BI_BLOCK) k_bi_true(BiArgs<MT, IT, VT> a, int 
   double v[2] = {0.0, 0.0};
   const int stride = gridDim.x * BI_BLOCK;
   for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) {
-    const double ax = sell_row(a.off, a.kd, a.su, a.wide_val, a.aval, a.ix, r, [&](int c) { return ldv(a.x + c); });
+    const double ax = a_row(a, r, [&](int c) { return ldv(a.x + c); });
     const double rt = a.b[r] - ax;
     if (replace) a.r[r] = rt;
     v[0] += (double)a.rs[r] * rt;
@@ -650,7 +729,8 @@ int grid_for(const Ctx* c, long long items, int per_sm, int sel) {
 
 template <typename MT, typename IT, typename VT>
 int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval, const IT* ix, const double* b,
-               double* x, const dcu_options* opt, const dcu_tuning* tu, dcu_solve_info* info) {
+               double* x, const dcu_options* opt, const dcu_tuning* tu, dcu_solve_info* info,
+               const MT* mval8 = nullptr) {
   const int n = plan.n;
   // blocks of each kernel resident on one SM at once
   auto resident = [&](const void* fn) {
@@ -711,10 +791,12 @@ int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval,
   a.n = n;
   a.off = plan.off;
   a.kd = plan.kd;
+  a.kd8 = plan.kd8;
   a.su = plan.su;
   a.ix = ix;
   a.aval = aval;
   a.mval = mval;
+  a.mval8 = mval8;
   a.b = b;
   a.x = x;
   a.r = (double*)(base);
@@ -902,7 +984,7 @@ int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval,
 }  // namespace
 
 int bicgstab_solve(Ctx* c, const SellPlan& plan, const double* aval_sell, const void* mval_sell, const double* b,
-                   double* x, const dcu_options* opt, dcu_solve_info* info) {
+                   double* x, const dcu_options* opt, dcu_solve_info* info, const void* mval8_sell) {
   const int p = opt->precision;
   const dcu_tuning* tu = (p >= 0 && p < 5 && c->tune_set[p]) ? &c->tune[p] : nullptr;
   if (p == DCU_PREC_FP64)
@@ -911,16 +993,18 @@ int bicgstab_solve(Ctx* c, const SellPlan& plan, const double* aval_sell, const 
   const bool v32 = (p == DCU_PREC_MIXED_FP32 || p == DCU_PREC_MIXED_BF16);
   const float* mf = (const float*)mval_sell;
   const __nv_bfloat16* mb = (const __nv_bfloat16*)mval_sell;
+  const float* mf8 = (const float*)mval8_sell;
+  const __nv_bfloat16* mb8 = (const __nv_bfloat16*)mval8_sell;
   if (plan.delta16) {
-    if (m32) return v32 ? run_solver<float, int16_t, float>(c, plan, aval_sell, mf, plan.del, b, x, opt, tu, info)
-                        : run_solver<float, int16_t, double>(c, plan, aval_sell, mf, plan.del, b, x, opt, tu, info);
-    return v32 ? run_solver<__nv_bfloat16, int16_t, float>(c, plan, aval_sell, mb, plan.del, b, x, opt, tu, info)
-               : run_solver<__nv_bfloat16, int16_t, double>(c, plan, aval_sell, mb, plan.del, b, x, opt, tu, info);
+    if (m32) return v32 ? run_solver<float, int16_t, float>(c, plan, aval_sell, mf, plan.del, b, x, opt, tu, info, mf8)
+                        : run_solver<float, int16_t, double>(c, plan, aval_sell, mf, plan.del, b, x, opt, tu, info, mf8);
+    return v32 ? run_solver<__nv_bfloat16, int16_t, float>(c, plan, aval_sell, mb, plan.del, b, x, opt, tu, info, mb8)
+               : run_solver<__nv_bfloat16, int16_t, double>(c, plan, aval_sell, mb, plan.del, b, x, opt, tu, info, mb8);
   }
-  if (m32) return v32 ? run_solver<float, int, float>(c, plan, aval_sell, mf, plan.idx, b, x, opt, tu, info)
-                      : run_solver<float, int, double>(c, plan, aval_sell, mf, plan.idx, b, x, opt, tu, info);
-  return v32 ? run_solver<__nv_bfloat16, int, float>(c, plan, aval_sell, mb, plan.idx, b, x, opt, tu, info)
-             : run_solver<__nv_bfloat16, int, double>(c, plan, aval_sell, mb, plan.idx, b, x, opt, tu, info);
+  if (m32) return v32 ? run_solver<float, int, float>(c, plan, aval_sell, mf, plan.idx, b, x, opt, tu, info, mf8)
+                      : run_solver<float, int, double>(c, plan, aval_sell, mf, plan.idx, b, x, opt, tu, info, mf8);
+  return v32 ? run_solver<__nv_bfloat16, int, float>(c, plan, aval_sell, mb, plan.idx, b, x, opt, tu, info, mb8)
+             : run_solver<__nv_bfloat16, int, double>(c, plan, aval_sell, mb, plan.idx, b, x, opt, tu, info, mb8);
 }
 
 namespace {

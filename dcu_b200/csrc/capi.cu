@@ -55,11 +55,13 @@ int resolve_range(Ctx* c, int n, const dcu_options* in, dcu_options* out) {
   return DCU_OK;
 }
 
-// A's values (FP64) and M's (by form) in SELL order.
+// A's values (FP64) and M's (by form) in SELL order; an FP32 / BF16 M's
+// narrow slices row-major in *msell8 (NULL for an FP64 M).
 int gather_values(Ctx* c, const dcu::SellPlan& pl, const double* val, const double* mval, int precision,
-                  const void** msell) {
+                  const void** msell, const void** msell8) {
   const dcu::SellPlan* plan = &pl;
   const size_t slots = (size_t)(plan->slots > 0 ? plan->slots : 1);
+  const size_t rows8 = (size_t)plan->nslices * 32 * dcu::kNarrow;
   DCU_TRY(dcu::ensure(c, dcu::B_SELL_AVAL, sizeof(double) * slots));
   DCU_TRY(dcu::sell_gather_f64(c, *plan, val, dcu::bp<double>(c, dcu::B_SELL_AVAL)));
   if (precision == DCU_PREC_FP64) {
@@ -67,20 +69,25 @@ int gather_values(Ctx* c, const dcu::SellPlan& pl, const double* val, const doub
     DCU_TRY(dcu::sell_gather_f64(c, *plan, mval, dcu::bp<double>(c, dcu::B_SELL_MVAL)));
   } else if (precision == DCU_PREC_MIXED_FP32 || precision == DCU_PREC_M_FP32) {
     DCU_TRY(dcu::ensure(c, dcu::B_SELL_MVAL, sizeof(float) * slots));
-    DCU_TRY(dcu::sell_gather_f32(c, *plan, mval, dcu::bp<float>(c, dcu::B_SELL_MVAL)));
+    DCU_TRY(dcu::ensure(c, dcu::B_SELL_MVAL8, sizeof(float) * rows8));
+    DCU_TRY(dcu::sell_gather_m8_f32(c, *plan, mval, dcu::bp<float>(c, dcu::B_SELL_MVAL),
+                                    dcu::bp<float>(c, dcu::B_SELL_MVAL8)));
   } else {
     DCU_TRY(dcu::ensure(c, dcu::B_SELL_MVAL, sizeof(__nv_bfloat16) * slots));
-    DCU_TRY(dcu::sell_gather_bf16(c, *plan, mval, dcu::bp<__nv_bfloat16>(c, dcu::B_SELL_MVAL)));
+    DCU_TRY(dcu::ensure(c, dcu::B_SELL_MVAL8, sizeof(__nv_bfloat16) * rows8));
+    DCU_TRY(dcu::sell_gather_m8_bf16(c, *plan, mval, dcu::bp<__nv_bfloat16>(c, dcu::B_SELL_MVAL),
+                                     dcu::bp<__nv_bfloat16>(c, dcu::B_SELL_MVAL8)));
   }
   *msell = c->buf[dcu::B_SELL_MVAL].p;
+  *msell8 = precision == DCU_PREC_FP64 ? nullptr : c->buf[dcu::B_SELL_MVAL8].p;
   return DCU_OK;
 }
 
 // Solver-side layout of A and M: SELL plan + values.
 int prepare_solve(Ctx* c, int n, int nnz, const int* ptr, const int* idx, const double* val, const double* mval,
-                  int precision, dcu::SellPlan* plan, const void** msell) {
+                  int precision, dcu::SellPlan* plan, const void** msell, const void** msell8) {
   DCU_TRY(dcu::sell_plan(c, n, nnz, ptr, idx, plan));
-  return gather_values(c, *plan, val, mval, precision, msell);
+  return gather_values(c, *plan, val, mval, precision, msell, msell8);
 }
 
 // The whole path on device arrays: validation, the SELL plan (pattern only),
@@ -106,10 +113,10 @@ int solve_pipeline(Ctx* c, int n, int nnz, const int* ptr, const int* idx, const
   DCU_CUDA(c, cudaEventRecord(c->ev[4], c->stream));
   DCU_TRY(dcu::spai_build(c, n, nnz, ptr, idx, val, &o, m, nullptr, &bl));
   DCU_CUDA(c, cudaEventRecord(c->ev[5], c->stream));
-  const void* msell = nullptr;
-  DCU_TRY(gather_values(c, plan, val, m, o.precision, &msell));
+  const void *msell = nullptr, *msell8 = nullptr;
+  DCU_TRY(gather_values(c, plan, val, m, o.precision, &msell, &msell8));
   if (bx_ready) DCU_CUDA(c, cudaStreamWaitEvent(c->stream, bx_ready, 0));
-  DCU_TRY(dcu::bicgstab_solve(c, plan, dcu::bp<double>(c, dcu::B_SELL_AVAL), msell, b, x, &o, sinfo));
+  DCU_TRY(dcu::bicgstab_solve(c, plan, dcu::bp<double>(c, dcu::B_SELL_AVAL), msell, b, x, &o, sinfo, msell8));
   DCU_CUDA(c, cudaEventSynchronize(c->ev[5]));
   cudaEventElapsedTime(&bl.ms, c->ev[4], c->ev[5]);
   if (binfo) *binfo = bl;
@@ -589,10 +596,10 @@ int dcu_bicgstab_d(dcu_spai_ctx* c, int n, int nnz, const int* ptr, const int* i
   try {
     StreamScope scope(c);
     dcu::SellPlan plan;
-    const void* msell = nullptr;
+    const void *msell = nullptr, *msell8 = nullptr;
     DCU_TRY(dcu::validate_csc(c, n, nnz, ptr, idx));
-    DCU_TRY(prepare_solve(c, n, nnz, ptr, idx, val, mval, o.precision, &plan, &msell));
-    return dcu::bicgstab_solve(c, plan, dcu::bp<double>(c, dcu::B_SELL_AVAL), msell, b, x, &o, info);
+    DCU_TRY(prepare_solve(c, n, nnz, ptr, idx, val, mval, o.precision, &plan, &msell, &msell8));
+    return dcu::bicgstab_solve(c, plan, dcu::bp<double>(c, dcu::B_SELL_AVAL), msell, b, x, &o, info, msell8);
   } catch (const std::bad_alloc&) {
     return dcu::fail(c, DCU_ERR_ALLOC, "host allocation failed");
   }
@@ -645,9 +652,9 @@ int dcu_bicgstab_transpose_d(dcu_spai_ctx* c, int n, int nnz, const int* ptr, co
     // A's CSC arrays are the CSR arrays of A^T (and of M^T: same pattern)
     dcu::SellPlan plan;
     DCU_TRY(dcu::sell_plan_rows(c, n, nnz, ptr, idx, &plan));
-    const void* msell = nullptr;
-    DCU_TRY(gather_values(c, plan, val, mval, o.precision, &msell));
-    return dcu::bicgstab_solve(c, plan, dcu::bp<double>(c, dcu::B_SELL_AVAL), msell, b, x, &o, info);
+    const void *msell = nullptr, *msell8 = nullptr;
+    DCU_TRY(gather_values(c, plan, val, mval, o.precision, &msell, &msell8));
+    return dcu::bicgstab_solve(c, plan, dcu::bp<double>(c, dcu::B_SELL_AVAL), msell, b, x, &o, info, msell8);
   } catch (const std::bad_alloc&) {
     return dcu::fail(c, DCU_ERR_ALLOC, "host allocation failed");
   }
@@ -694,8 +701,8 @@ int dcu_batch_solve_d(dcu_spai_ctx* c, int nsys, const int* sys_off, int n, int 
     cudaEventElapsedTime(&bl.ms, c->ev[0], c->ev[1]);
     if (binfo) *binfo = bl;
     dcu::SellPlan plan;
-    const void* msell = nullptr;
-    DCU_TRY(prepare_solve(c, n, nnz, ptr, idx, val, m, DCU_PREC_FP64, &plan, &msell));
+    const void *msell = nullptr, *msell8 = nullptr;
+    DCU_TRY(prepare_solve(c, n, nnz, ptr, idx, val, m, DCU_PREC_FP64, &plan, &msell, &msell8));
     return dcu::batch_solve(c, nsys, sys_off, plan, dcu::bp<double>(c, dcu::B_SELL_AVAL), (const double*)msell,
                             nrhs, B, X, &o, iters, status, sinfo);
   } catch (const std::bad_alloc&) {

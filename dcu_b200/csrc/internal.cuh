@@ -57,6 +57,8 @@ enum BufId {
   B_HUBWPRE,       // prefix of their widths (warp -> column map)
   B_SELL_WIDE,     // SELL: count and list of the slices wider than kWideSlice
   B_WIDEVAL,       // solver: row values of those slices, from the wide pre-pass
+  B_SELL_KD8,      // SELL: per narrow slice, its (up to 8) column offsets
+  B_SELL_MVAL8,    // M values (FP32 / BF16) of the narrow slices, 8 per row, row-major
   B_COUNT
 };
 
@@ -161,6 +163,11 @@ int scan_exclusive_i64(Ctx* c, const int* in, long long* out, int n);
 // keep the per-lane loop, which serves them better.
 constexpr int kWideSlice = 16;
 constexpr int kWideRows = 4;
+// Offset-uniform slices at most this wide are "narrow" (every slice of a 5-
+// or 7-point stencil): their offsets are kept per slice (SellPlan::kd8) and,
+// for an FP32 / BF16 M, their values row-major, kNarrow per row, so one
+// vector load brings a row's values.
+constexpr int kNarrow = 8;
 
 struct SellPlan {
   int n = 0, nnz = 0;
@@ -176,10 +183,17 @@ struct SellPlan {
   // row of the slice has its k-th entry at column row + d, else 0.  A warp
   // then forms the column from the row and skips the per-slot index load.
   const int* kd = nullptr;
-  // Per slice: bit 0 when every kd of the slice is uniform; bit 2 when the
-  // slice is full, wider than kWideSlice and has at most kWideRows rows
-  // longer than that, with its index in `wide` in the bits above bit 2.
+  // Per slice: bit 0 when every kd of the slice is uniform; bit 1 when, in
+  // addition, the slice is at most kNarrow slots wide ("narrow"), with its
+  // width in bits 3-6; bit 2 when the slice is full, wider than kWideSlice and
+  // has at most kWideRows rows longer than that, with its index in `wide` in
+  // the bits above bit 2.
   const int* su = nullptr;
+  // kNarrow ints per slice: kd8[kNarrow s + k] = the column offset of entry
+  // position k of a narrow slice (0 past its width).  Indexed by the slice
+  // alone, so a row's offsets load together with its slice's flags instead
+  // of after its slot offset.
+  const int* kd8 = nullptr;
   const int* rptr = nullptr;  // CSR row pointers of the laid-out operator (row lengths)
   const int* wide = nullptr;  // the slices flagged wide (device)
   int nwide = 0;
@@ -208,6 +222,11 @@ int sampled_outer(Ctx* c, int n, const int* ptr, const int* idx, const double* u
 int sell_gather_f64(Ctx* c, const SellPlan& p, const double* src, double* dst);
 int sell_gather_f32(Ctx* c, const SellPlan& p, const double* src, float* dst);
 int sell_gather_bf16(Ctx* c, const SellPlan& p, const double* src, __nv_bfloat16* dst);
+// An FP32 / BF16 M for the solver: the values of the narrow slices row-major,
+// kNarrow per row (dst8, nslices * 32 * kNarrow), the other slices' values in
+// SELL order (dst, slots).
+int sell_gather_m8_f32(Ctx* c, const SellPlan& p, const double* src, float* dst, float* dst8);
+int sell_gather_m8_bf16(Ctx* c, const SellPlan& p, const double* src, __nv_bfloat16* dst, __nv_bfloat16* dst8);
 
 // ---------------------------------------------------------------------------
 // SPAI build and pattern.
@@ -223,8 +242,11 @@ int spai_pattern(Ctx* c, int n, const int* ptr, const int* idx, int col_start, i
 // ---------------------------------------------------------------------------
 // BiCGSTAB on the SELL plan.
 // ---------------------------------------------------------------------------
+// mval8_sell: an FP32 / BF16 M's narrow-slice values (sell_gather_m8_*), or
+// NULL (every slice then read from mval_sell).
 int bicgstab_solve(Ctx* c, const SellPlan& plan, const double* aval_sell, const void* mval_sell,
-                   const double* b, double* x, const dcu_options* opt, dcu_solve_info* info);
+                   const double* b, double* x, const dcu_options* opt, dcu_solve_info* info,
+                   const void* mval8_sell = nullptr);
 void release_graphs(Ctx* c);
 
 // Batched systems (diagonal blocks [sys_off[s], sys_off[s+1]) of one matrix).

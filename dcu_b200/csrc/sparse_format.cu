@@ -289,28 +289,36 @@ __global__ void k_sell_delta(const int* __restrict__ sidx, long long slots, int 
 // whether all of the slice's rows below n have their k-th slot at the same
 // offset d = column - row.  Rows past n (last slice) never run and do not
 // count.  Writes kd[off[s] / 32 + k] = (d << 1) | 1, or 0, and su[s] = 1 when
-// every k of the slice has one offset (the SpMV then reads no index at all).
+// every k of the slice has one offset (the SpMV then reads no index at all);
+// for such a slice at most kNarrow wide also the narrow flag, its width and
+// kd8[kNarrow s + k] = d (the SellPlan::su bits).
 __global__ void k_sell_desc(const int* __restrict__ sidx, int n, int nslices, const long long* __restrict__ off,
                             int* __restrict__ kd, int* __restrict__ su, unsigned long long* __restrict__ uslots,
-                            const int* __restrict__ rptr, int* __restrict__ wide, int allow_wide) {
+                            const int* __restrict__ rptr, int* __restrict__ wide, int allow_wide,
+                            int* __restrict__ kd8) {
   const int rows_total = nslices * 32;
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows_total; r += gridDim.x * blockDim.x) {
     const int s = r >> 5, lane = r & 31;
     const long long o0 = off[s];
     const int w = (int)((off[s + 1] - o0) >> 5);
     bool all = true;
+    int my_d = 0;  // lane k < kNarrow: offset of entry position k
     for (int k = 0; k < w; ++k) {
       const int d = sidx[o0 + 32ll * k + lane] - r;
       const int d0 = __shfl_sync(0xffffffffu, d, 0);  // row 32 s < n always
       const bool same = __all_sync(0xffffffffu, r >= n || d == d0);
       all = all && same;
       if (lane == 0) kd[(o0 >> 5) + k] = same ? (int)(((unsigned)d0 << 1) | 1u) : 0;
+      if (lane == k) my_d = d0;
     }
+    const bool narrow = all && w > 0 && w <= kNarrow;
+    if (lane < kNarrow) kd8[(long long)s * kNarrow + lane] = (narrow && lane < w) ? my_d : 0;
     // rows of the slice longer than kWideSlice
     const int len = (r < n) ? rptr[r + 1] - rptr[r] : 0;
     const int nlong = __popc(__ballot_sync(0xffffffffu, len > kWideSlice));
     if (lane == 0) {
       int f = all ? 1 : 0;
+      if (narrow) f |= 2 | (w << 3);
       // a full slice made wide by a few long rows: listed for the solver's
       // pre-pass (wide[0] counts, wide[1 + i] = slice)
       if (allow_wide && w > kWideSlice && nlong <= kWideRows && 32 * s + 32 <= n) {
@@ -571,10 +579,12 @@ int sell_fill_from_csr(Ctx* c, int n, int nnz, const int* rptr, const int* rcol,
   DCU_CUDA(c, cudaMemcpyAsync(pst, hst, sizeof(hst), cudaMemcpyHostToDevice, c->stream));
   DCU_TRY(ensure(c, B_SELL_WIDE, sizeof(int) * ((size_t)nslices + 1)));
   int* wide = bp<int>(c, B_SELL_WIDE);
+  DCU_TRY(ensure(c, B_SELL_KD8, sizeof(int) * kNarrow * (size_t)nslices));
+  int* kd8 = bp<int>(c, B_SELL_KD8);
   DCU_CUDA(c, cudaMemsetAsync(wide, 0, sizeof(int), c->stream));
   k_sell_desc<<<waves_grid(c, (long long)nslices * 32, 256, 8), 256, 0, c->stream>>>(sidx, n, nslices, off, kd, su,
                                                                                        pst + 1, rptr, wide,
-                                                                                       c->wide_prepass ? 1 : 0);
+                                                                                       c->wide_prepass ? 1 : 0, kd8);
   DCU_LAUNCHED(c, "k_sell_desc");
   DCU_CUDA(c, cudaMemcpyAsync(c->pinned, wide, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   DCU_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -583,6 +593,7 @@ int sell_fill_from_csr(Ctx* c, int n, int nnz, const int* rptr, const int* rcol,
   plan->wide = wide + 1;
   plan->rptr = rptr;
   plan->kd = kd;
+  plan->kd8 = kd8;
   plan->su = su;
   plan->n = n;
   plan->nnz = nnz;
@@ -624,6 +635,68 @@ int sell_gather_f64(Ctx* c, const SellPlan& p, const double* src, double* dst) {
 int sell_gather_f32(Ctx* c, const SellPlan& p, const double* src, float* dst) { return sell_gather<float>(c, p, src, dst); }
 int sell_gather_bf16(Ctx* c, const SellPlan& p, const double* src, __nv_bfloat16* dst) {
   return sell_gather<__nv_bfloat16>(c, p, src, dst);
+}
+
+namespace {
+
+// kNarrow values of one row, stored with one (BF16: 16 bytes) or two (FP32:
+// 2 x 16 bytes) vector stores.
+__device__ __forceinline__ void store_row8(__nv_bfloat16* p, const double (&v)[kNarrow]) {
+  __nv_bfloat162 h[kNarrow / 2];
+#pragma unroll
+  for (int k = 0; k < kNarrow / 2; ++k) h[k] = __halves2bfloat162(__double2bfloat16(v[2 * k]), __double2bfloat16(v[2 * k + 1]));
+  *reinterpret_cast<uint4*>(p) = *reinterpret_cast<const uint4*>(h);
+}
+__device__ __forceinline__ void store_row8(float* p, const double (&v)[kNarrow]) {
+  reinterpret_cast<float4*>(p)[0] = make_float4((float)v[0], (float)v[1], (float)v[2], (float)v[3]);
+  reinterpret_cast<float4*>(p)[1] = make_float4((float)v[4], (float)v[5], (float)v[6], (float)v[7]);
+}
+
+// One thread per row of the layout: a narrow slice's row goes to dst8 (its
+// kNarrow values, zeros past the width), any other row to its SELL slots.
+template <typename T>
+__global__ void k_sell_gather_m8(const long long* __restrict__ off, const int* __restrict__ su,
+                                 const int* __restrict__ sperm, int nslices, const double* __restrict__ src,
+                                 T* __restrict__ dst, T* __restrict__ dst8) {
+  const int rows_total = nslices * 32;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows_total; r += gridDim.x * blockDim.x) {
+    const int s = r >> 5, lane = r & 31;
+    const long long o0 = off[s];
+    const int w = (int)((off[s + 1] - o0) >> 5);
+    const long long base = o0 + lane;
+    if (su[s] & 2) {
+      double v[kNarrow];
+#pragma unroll
+      for (int k = 0; k < kNarrow; ++k) {
+        const int p = (k < w) ? sperm[base + 32ll * k] : -1;
+        v[k] = p >= 0 ? src[p] : 0.0;
+      }
+      store_row8(dst8 + (long long)r * kNarrow, v);
+    } else {
+      for (int k = 0; k < w; ++k) {
+        const long long q = base + 32ll * k;
+        const int p = sperm[q];
+        dst[q] = cvt_from_double<T>(p >= 0 ? src[p] : 0.0);
+      }
+    }
+  }
+}
+
+template <typename T>
+int sell_gather_m8(Ctx* c, const SellPlan& p, const double* src, T* dst, T* dst8) {
+  k_sell_gather_m8<T><<<waves_grid(c, (long long)p.nslices * 32, 256, 8), 256, 0, c->stream>>>(
+      p.off, p.su, p.perm, p.nslices, src, dst, dst8);
+  DCU_LAUNCHED(c, "k_sell_gather_m8");
+  return DCU_OK;
+}
+
+}  // namespace
+
+int sell_gather_m8_f32(Ctx* c, const SellPlan& p, const double* src, float* dst, float* dst8) {
+  return sell_gather_m8<float>(c, p, src, dst, dst8);
+}
+int sell_gather_m8_bf16(Ctx* c, const SellPlan& p, const double* src, __nv_bfloat16* dst, __nv_bfloat16* dst8) {
+  return sell_gather_m8<__nv_bfloat16>(c, p, src, dst, dst8);
 }
 
 // CSR with values, for the C ABI (dcu_csc_to_csr_d).
