@@ -106,15 +106,46 @@ struct Row8<double> {  // never loaded: an FP64 M has no narrow array
 // one for its gathers.  Every path sums the row's products in entry order.
 // The rows of a slice that the plan flagged wide (su bit 2) were summed by
 // the wide pre-pass (k_bi_wide) into wv.
+// A narrow slice's kNarrow offsets: int16 (one 16-byte load) with 16-bit
+// column deltas, else int32 (two).
+template <typename IT>
+struct Kd8 {
+  int4 a, b;
+  __device__ __forceinline__ void load(const int* kd8, const int16_t*, int s) {
+    const int4* q = reinterpret_cast<const int4*>(kd8 + (long long)s * kNarrow);
+    a = __ldg(q);
+    b = __ldg(q + 1);
+  }
+  __device__ __forceinline__ void unpack(int (&d)[kNarrow]) const {
+    d[0] = a.x; d[1] = a.y; d[2] = a.z; d[3] = a.w; d[4] = b.x; d[5] = b.y; d[6] = b.z; d[7] = b.w;
+  }
+};
+template <>
+struct Kd8<int16_t> {
+  int4 a;
+  __device__ __forceinline__ void load(const int*, const int16_t* kd8h, int s) {
+    a = __ldg(reinterpret_cast<const int4*>(kd8h + (long long)s * kNarrow));
+  }
+  __device__ __forceinline__ void unpack(int (&d)[kNarrow]) const {
+    const int w[4] = {a.x, a.y, a.z, a.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      d[2 * k] = (int)(short)(w[k] & 0xffff);
+      d[2 * k + 1] = w[k] >> 16;
+    }
+  }
+};
+
 template <bool M8, typename MT, typename IT, typename F>
 __device__ __forceinline__ double sell_row(const long long* __restrict__ off, const int* __restrict__ kd,
-                                           const int* __restrict__ kd8, const int* __restrict__ su,
-                                           const double* __restrict__ wv, const MT* __restrict__ val,
-                                           const MT* __restrict__ val8, const IT* __restrict__ ix, int r, F xf) {
+                                           const int* __restrict__ kd8, const int16_t* __restrict__ kd8h,
+                                           const int* __restrict__ su, const double* __restrict__ wv,
+                                           const MT* __restrict__ val, const MT* __restrict__ val8,
+                                           const IT* __restrict__ ix, int r, F xf) {
   const int s = r >> 5;
   const int f = __ldg(su + s);
-  const int4* kq = reinterpret_cast<const int4*>(kd8 + (long long)s * kNarrow);
-  const int4 da = __ldg(kq), db = __ldg(kq + 1);
+  Kd8<IT> kq;
+  kq.load(kd8, kd8h, s);
   Row8<MT> m8;
   long long o0 = 0, o1 = 0;
   if (M8) {
@@ -126,7 +157,8 @@ __device__ __forceinline__ double sell_row(const long long* __restrict__ off, co
   if (f & 4) return __ldg(wv + ((long long)(f >> 3) << 5) + (r & 31));
   if (f & 2) {
     const int w = (f >> 3) & 15;
-    const int d[kNarrow] = {da.x, da.y, da.z, da.w, db.x, db.y, db.z, db.w};
+    int d[kNarrow];
+    kq.unpack(d);
     double av[kNarrow];
     const long long base = o0 + (r & 31);
 #pragma unroll
@@ -241,6 +273,7 @@ struct BiArgs {
   const long long* off;
   const int* kd;        // per (slice, k) offset descriptors (SellPlan::kd)
   const int* kd8;       // per narrow slice, its offsets (SellPlan::kd8)
+  const int16_t* kd8h;  // the same as int16 (with 16-bit column deltas)
   const int* su;        // per slice flags (SellPlan::su)
   const IT* ix;         // shared by A and M (same pattern)
   const double* aval;
@@ -268,14 +301,15 @@ struct BiArgs {
 // A's row (FP64 values in SELL order).
 template <typename MT, typename IT, typename VT, typename F>
 __device__ __forceinline__ double a_row(const BiArgs<MT, IT, VT>& a, int r, F xf) {
-  return sell_row<false, double, IT>(a.off, a.kd, a.kd8, a.su, a.wide_val, a.aval, nullptr, a.ix, r, xf);
+  return sell_row<false, double, IT>(a.off, a.kd, a.kd8, a.kd8h, a.su, a.wide_val, a.aval, nullptr, a.ix, r, xf);
 }
 // M's row: narrow slices from the row-major narrow array where the form has one.
 template <typename MT, typename IT, typename VT, typename F>
 __device__ __forceinline__ double m_row(const BiArgs<MT, IT, VT>& a, int r, F xf) {
   constexpr bool narrow = !std::is_same<MT, double>::value;
-  if (narrow && a.mval8) return sell_row<narrow, MT, IT>(a.off, a.kd, a.kd8, a.su, a.wide_val, a.mval, a.mval8, a.ix, r, xf);
-  return sell_row<false, MT, IT>(a.off, a.kd, a.kd8, a.su, a.wide_val, a.mval, nullptr, a.ix, r, xf);
+  if (narrow && a.mval8)
+    return sell_row<narrow, MT, IT>(a.off, a.kd, a.kd8, a.kd8h, a.su, a.wide_val, a.mval, a.mval8, a.ix, r, xf);
+  return sell_row<false, MT, IT>(a.off, a.kd, a.kd8, a.kd8h, a.su, a.wide_val, a.mval, nullptr, a.ix, r, xf);
 }
 
 // Kernels K1..K5 are launched with programmatic dependent launch: their blocks
@@ -792,6 +826,7 @@ int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval,
   a.off = plan.off;
   a.kd = plan.kd;
   a.kd8 = plan.kd8;
+  a.kd8h = plan.kd8h;
   a.su = plan.su;
   a.ix = ix;
   a.aval = aval;

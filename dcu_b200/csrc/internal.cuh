@@ -57,7 +57,7 @@ enum BufId {
   B_HUBWPRE,       // prefix of their widths (warp -> column map)
   B_SELL_WIDE,     // SELL: count and list of the slices wider than kWideSlice
   B_WIDEVAL,       // solver: row values of those slices, from the wide pre-pass
-  B_SELL_KD8,      // SELL: per narrow slice, its (up to 8) column offsets
+  B_SELL_KD8,      // SELL: per narrow slice, its (up to 8) column offsets (int32, then int16)
   B_SELL_MVAL8,    // M values (FP32 / BF16) of the narrow slices, 8 per row, row-major
   B_COUNT
 };
@@ -194,6 +194,8 @@ struct SellPlan {
   // alone, so a row's offsets load together with its slice's flags instead
   // of after its slot offset.
   const int* kd8 = nullptr;
+  // the same offsets as int16 (one 16-byte load per slice) when delta16
+  const int16_t* kd8h = nullptr;
   const int* rptr = nullptr;  // CSR row pointers of the laid-out operator (row lengths)
   const int* wide = nullptr;  // the slices flagged wide (device)
   int nwide = 0;

@@ -295,7 +295,7 @@ __global__ void k_sell_delta(const int* __restrict__ sidx, long long slots, int 
 __global__ void k_sell_desc(const int* __restrict__ sidx, int n, int nslices, const long long* __restrict__ off,
                             int* __restrict__ kd, int* __restrict__ su, unsigned long long* __restrict__ uslots,
                             const int* __restrict__ rptr, int* __restrict__ wide, int allow_wide,
-                            int* __restrict__ kd8) {
+                            int* __restrict__ kd8, int16_t* __restrict__ kd8h) {
   const int rows_total = nslices * 32;
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows_total; r += gridDim.x * blockDim.x) {
     const int s = r >> 5, lane = r & 31;
@@ -312,7 +312,11 @@ __global__ void k_sell_desc(const int* __restrict__ sidx, int n, int nslices, co
       if (lane == k) my_d = d0;
     }
     const bool narrow = all && w > 0 && w <= kNarrow;
-    if (lane < kNarrow) kd8[(long long)s * kNarrow + lane] = (narrow && lane < w) ? my_d : 0;
+    if (lane < kNarrow) {
+      const int d = (narrow && lane < w) ? my_d : 0;
+      kd8[(long long)s * kNarrow + lane] = d;
+      if (kd8h) kd8h[(long long)s * kNarrow + lane] = (int16_t)d;  // |d| < 32768 (delta16)
+    }
     // rows of the slice longer than kWideSlice
     const int len = (r < n) ? rptr[r + 1] - rptr[r] : 0;
     const int nlong = __popc(__ballot_sync(0xffffffffu, len > kWideSlice));
@@ -579,12 +583,13 @@ int sell_fill_from_csr(Ctx* c, int n, int nnz, const int* rptr, const int* rcol,
   DCU_CUDA(c, cudaMemcpyAsync(pst, hst, sizeof(hst), cudaMemcpyHostToDevice, c->stream));
   DCU_TRY(ensure(c, B_SELL_WIDE, sizeof(int) * ((size_t)nslices + 1)));
   int* wide = bp<int>(c, B_SELL_WIDE);
-  DCU_TRY(ensure(c, B_SELL_KD8, sizeof(int) * kNarrow * (size_t)nslices));
+  DCU_TRY(ensure(c, B_SELL_KD8, (sizeof(int) + sizeof(int16_t)) * kNarrow * (size_t)nslices));
   int* kd8 = bp<int>(c, B_SELL_KD8);
+  int16_t* kd8h = plan->delta16 ? reinterpret_cast<int16_t*>(kd8 + kNarrow * (size_t)nslices) : nullptr;
   DCU_CUDA(c, cudaMemsetAsync(wide, 0, sizeof(int), c->stream));
   k_sell_desc<<<waves_grid(c, (long long)nslices * 32, 256, 8), 256, 0, c->stream>>>(sidx, n, nslices, off, kd, su,
                                                                                        pst + 1, rptr, wide,
-                                                                                       c->wide_prepass ? 1 : 0, kd8);
+                                                                                       c->wide_prepass ? 1 : 0, kd8, kd8h);
   DCU_LAUNCHED(c, "k_sell_desc");
   DCU_CUDA(c, cudaMemcpyAsync(c->pinned, wide, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   DCU_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -594,6 +599,7 @@ int sell_fill_from_csr(Ctx* c, int n, int nnz, const int* rptr, const int* rcol,
   plan->rptr = rptr;
   plan->kd = kd;
   plan->kd8 = kd8;
+  plan->kd8h = kd8h;
   plan->su = su;
   plan->n = n;
   plan->nnz = nnz;
