@@ -12,11 +12,12 @@
 //   M(J_k, k) = m_k                                  (modifyData4_SSPAIv10 :1135-1152)
 //
 // Two kernels share the column range through a device work queue:
-//   k_spai_small  one 8-lane group per column, |J_k| <= 7, <= 64 candidate
-//                 rows, |I_k| <= 32 (or the tuned group_max_ni below it):
-//                 candidates sorted in registers (bitonic
-//                 network across the group), At staged in shared memory, one
-//                 lane per column of [At | e_E] holding it in registers.
+//   k_spai_small  one 16-lane group per column (two per warp), |J_k| <= 7,
+//                 <= 64 candidate rows, |I_k| <= 32 (or the tuned
+//                 group_max_ni below it): candidates sorted in registers
+//                 (bitonic network across the group), At staged in shared
+//                 memory, two lanes per column of [At | e_E], each holding
+//                 half its rows in registers.
 //   k_spai_large  one CTA per column for everything else: I_k by a bitmap
 //                 over the candidate row range, At in shared memory or a
 //                 global slab, Householder with warp-per-trailing-column
@@ -171,10 +172,12 @@ __device__ __forceinline__ bool group_qr_solve(const SmallArgs& a, WarpSmem<T>& 
 #pragma unroll
   for (int c = 0; c < SG_NJMAX; ++c) {
     if (c >= steps) break;
-    // both lanes of column c: norm of rows >= c, reflector, R_cc
-    T part = T(0);
+    // both lanes of column c: norm of rows >= c (two independent partial
+    // sums: a shorter dependent chain), reflector, R_cc
+    T pp[2] = {T(0), T(0)};
 #pragma unroll
-    for (int t = 0; t < RPL; ++t) part += (row0 + t >= c) ? r[t] * r[t] : T(0);
+    for (int t = 0; t < RPL; ++t) pp[t & 1] += (row0 + t >= c) ? r[t] * r[t] : T(0);
+    T part = pp[0] + pp[1];
     part += __shfl_xor_sync(gmask, part, 1, GL);
     const T nrm2 = __shfl_sync(gmask, part, 2 * c, GL);
     const T x0 = __shfl_sync(gmask, r[c], 2 * c, GL);  // row c < RPL: first half
@@ -200,15 +203,12 @@ __device__ __forceinline__ bool group_qr_solve(const SmallArgs& a, WarpSmem<T>& 
     // v is re-read from shared memory in both loops (volatile) rather than
     // held in RPL more registers: fewer registers, more resident problems
     const volatile T* vv = v + row0;
-    T w0 = T(0), w1 = T(0);
+    T wp[2] = {T(0), T(0)};
     if (trailing) {
 #pragma unroll
-      for (int t = 0; t < RPL; ++t) {
-        if (t & 1) w1 += vv[t] * r[t];
-        else w0 += vv[t] * r[t];
-      }
+      for (int t = 0; t < RPL; ++t) wp[t & 1] += vv[t] * r[t];
     }
-    T w = w0 + w1;
+    T w = wp[0] + wp[1];
     w += __shfl_xor_sync(gmask, w, 1, GL);
     if (trailing) {
       w *= beta;
@@ -238,15 +238,17 @@ __device__ __forceinline__ bool group_qr_solve(const SmallArgs& a, WarpSmem<T>& 
   }
   res2 += __shfl_xor_sync(gmask, res2, 1, GL);
   __syncwarp(gmask);
-  if (lane == 0) {
-    for (int i = nj - 1; i >= 0; --i) {
-      T xi = v[i];
-      for (int jc = i + 1; jc < nj; ++jc) xi -= ws.At[g][jc][i] * v[jc];
-      v[i] = xi * ws.dinv[g][i];
-    }
+  // R x = y, column by column: lane i holds y_i; at step jc lane jc's x_jc
+  // is final, goes to every lane, and the lanes above it subtract its column
+  // (one shuffle per step instead of one lane walking the whole triangle)
+  T yi = (lane < nj) ? v[lane] : T(0);
+  const T di = (lane < nj) ? ws.dinv[g][lane] : T(0);
+  for (int jc = nj - 1; jc >= 0; --jc) {
+    const T xj = __shfl_sync(gmask, yi * di, jc, GL);
+    if (lane < jc) yi -= ws.At[g][jc][lane] * xj;
+    else if (lane == jc) yi = xj;
   }
-  __syncwarp(gmask);
-  if (lane < nj) a.mval[cs + lane] = (double)v[lane];
+  if (lane < nj) a.mval[cs + lane] = (double)yi;
   if (j == nj && h == 0 && a.colres) a.colres[k - a.col_start] = sqrt((double)res2);
   const unsigned any_sing = __ballot_sync(gmask, sing) & gmask;
   __syncwarp(gmask);
@@ -324,8 +326,10 @@ __device__ __forceinline__ int group_column(const SmallArgs& a, WarpSmem<T>& ws,
   }
   if (lane == 0 && E >= 0) ws.At[g][nj][E] = T(1);
   __syncwarp(gmask);
+  // row tiles of 16, 26 (a 3D 7-point column has |I| = 25) or 32 rows
   const bool sing = (m < nj) | ((m <= 16) ? group_qr_solve<16, T>(a, ws, g, lane, gmask, k, cs, nj, m)
-                                          : group_qr_solve<32, T>(a, ws, g, lane, gmask, k, cs, nj, m));
+                                : (m <= 26) ? group_qr_solve<26, T>(a, ws, g, lane, gmask, k, cs, nj, m)
+                                            : group_qr_solve<32, T>(a, ws, g, lane, gmask, k, cs, nj, m));
   if (sing && lane == 0) atomicAdd(&a.stats[ST_SINGULAR], 1);
   return m;
 }
