@@ -15,12 +15,14 @@ Synthetic seeded data; the reference publishes no number for it.
          precision forms are compared with), measured in the same run
 
 python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                [--workload cd3d128|batch512|grad512]
+                [--workload cd3d128|batch512|grad512|shard]
 Under torchrun each rank solves its own copy (replicas; weak scaling, no
 collective on the data path); ms is the max over ranks.  batch512 (512
 stencil systems x 8 right-hand sides, batched solver) and grad512 (512^2
-variable-coefficient diffusion, forward solve + adjoint gradient) print their
-own lines; the default workload is the headline.
+variable-coefficient diffusion, forward solve + adjoint gradient) and shard
+(the 128^3 SPAI build split by columns over the ranks, M all-gathered over
+NCCL; strong scaling) print their own lines; the default workload is the
+headline.
 """
 from __future__ import annotations
 
@@ -277,14 +279,150 @@ def run_extra(args, rank, world):
         ai = ctx.last_adjoint
         cfg.update({"forward_iters": si.iters, "forward_build_ms": round(bi.ms, 3), "forward_solve_ms": round(si.ms, 3),
                     "adjoint_iters": ai.iters, "adjoint_solve_ms": round(ai.ms, 3)})
+        # algorithmic bytes of one step: the FP64 SPAI build (A read once, M
+        # written), forward and adjoint iterations at the FP64 form's
+        # per-iteration bytes (fused first step, the form's default), and the
+        # sampled outer product (u, v read, 8 bytes written per entry)
+        n, z = Av.n, Av.nnz
+        slots, uslots = ctx.sell_plan_stats()
+        it_b = sum(bytes_per_kernel(n, z, 8, 8, index_bytes(n, 4, slots, uslots), False))
+        total = 12 * z + 4 * (n + 1) + 8 * z + (si.iters + ai.iters) * it_b + 8 * z + 16 * n
+        peaks = {}
+        try:
+            peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        except OSError:
+            pass
+        peak = float(peaks.get("hbm_gbs", 6650.0))
+        gbs = total / (v * 1e-3) / 1e9
+        roofline = {"bound": "hbm", "scope": "whole step (build + forward + adjoint + sampled outer product), "
+                    "algorithmic bytes", "bytes": int(total), "iteration_bytes": int(it_b), "achieved": round(gbs, 1),
+                    "peak": peak, "unit": "GB/s", "frac": round(gbs / peak, 3),
+                    "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                    "note": "262,144 rows: each of the ten kernels of an iteration is a short dependent chain "
+                            "(launch- and latency-bound, not bandwidth-bound)"}
+    cpu = None
+    if not args.no_cpu_baseline:
+        import oracle
+
+        threads = os.cpu_count() or 1
+        oracle.set_threads(threads)
+        t0 = time.perf_counter()
+        if args.workload == "grad512":
+            m_o, _, _, _ = oracle.spai(Av, "mgs")
+            bh, xth = b.cpu().numpy(), xt.cpu().numpy()
+            r = oracle.bicgstab(Av, m_o, bh, None, tol=1e-8, tol_mode="rel", maxiter=3000)
+            g = 2.0 * (r["x"] - xth)
+            rp, ri, rv = oracle.csc2csr(Av.n, Av.ptr, Av.idx, Av.val)
+            mt = oracle.csc2csr(Av.n, Av.ptr, Av.idx, m_o)[2]
+            ra = oracle.bicgstab(W.CSC(Av.n, rp, ri, rv), mt, g, None, tol=1e-8, tol_mode="rel", maxiter=3000)
+            cms = (time.perf_counter() - t0) * 1e3
+            cpu = {"value": round(cms, 1), "unit": "ms", "cores": threads, "kind": "port",
+                   "sample": f"full workload once (MGS SPAI, forward {r['iters']} and adjoint {ra['iters']} "
+                             "iterations of the reference-order BiCGSTAB; the sampled outer product not included)"}
+        else:
+            # the first 64 of the 512 systems, scaled to the whole batch by rows
+            ns = 64
+            off = bt.offsets.astype(np.int64)
+            for s in range(ns):
+                s0, s1 = int(off[s]), int(off[s + 1])
+                sub_ptr = (A.ptr[s0:s1 + 1] - A.ptr[s0]).astype(np.int32)
+                As = W.CSC(s1 - s0, sub_ptr, (A.idx[A.ptr[s0]:A.ptr[s1]] - s0).astype(np.int32),
+                           A.val[A.ptr[s0]:A.ptr[s1]])
+                m_s, _, _, _ = oracle.spai(As, "mgs")
+                for q in range(bt.B.shape[1]):
+                    oracle.bicgstab(As, m_s, bt.B[s0:s1, q], None, tol=1e-8, tol_mode="rel", maxiter=1000)
+            cms = (time.perf_counter() - t0) * 1e3
+            scale = float(off[-1]) / float(off[ns])
+            cpu = {"value": round(cms * scale, 1), "unit": "ms", "cores": threads, "kind": "port",
+                   "sample": f"first {ns} of {len(off) - 1} systems x {bt.B.shape[1]} rhs (MGS SPAI + "
+                             f"reference-order BiCGSTAB per pair): {cms:.1f} ms, scaled by rows x{scale:.2f}"}
     line = {"metric": metric, "value": round(v, 3), "unit": "ms", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(v, 3), "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg}
     if roofline:
         line["roofline"] = roofline
+    if cpu:
+        line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
     ctx.close()
     return 0
+
+
+def run_shard(args, rank, world, local):
+    """--workload shard: the column-sharded SPAI build of the 128^3 matrix
+    (plain FP64 Householder form) over N GPUs: each rank builds its
+    distributeColumns range and one NCCL all-gather assembles M on every rank.
+    Total work is fixed (strong scaling); ms is the max over ranks."""
+    import datetime
+
+    import torch
+
+    from dcu_b200 import native as N
+    from dcu_b200 import parallel
+    from dcu_b200.api import Context
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    A, _, _ = workload()
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    ptr, idx, val = t(A.ptr), t(A.idx), t(A.val)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    ctx = Context(local)
+    stream = torch.cuda.current_stream(dev)
+    ctx.set_stream(stream.cuda_stream)
+    build = parallel.device_slice_builder(ctx, A.n, A.nnz, ptr, idx, val, A.ptr, precision=N.PREC_FP64)
+
+    def step():
+        return parallel.sharded_build(build, A.ptr, A.n, rank, world, N.SCHED_BALANCED_NNZ)
+
+    for _ in range(args.warmup):
+        m = step()
+    torch.cuda.synchronize(dev)
+    ms = []
+    launches0 = ctx.launches
+    for i in range(args.steps):
+        flush.fill_(float(i))
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        m = step()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        ms.append(e0.elapsed_time(e1))
+    launches = ctx.launches - launches0
+    v = statistics.mean(ms)
+    if dist is not None:
+        tt = torch.tensor([v], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        v = float(tt.item())
+    # M equals one whole build bit for bit (checked outside the timed region)
+    whole = torch.zeros(A.nnz, dtype=torch.float64, device=dev)
+    ctx.build_d(A.n, A.nnz, ptr, idx, val, whole, precision=N.PREC_FP64)
+    same = bool(torch.equal(whole, m))
+    if rank == 0:
+        line = {"metric": "column-sharded SPAI build ms (128^3 convection-diffusion, FP64 Householder, M "
+                          "assembled on every rank)", "value": round(v, 3), "unit": "ms", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(v, 3), "higher_is_better": False,
+                "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": "convdiff3d 128^3 Pe 20: SPAI columns split by distributeColumns "
+                                       "(balanced_nnz) over the ranks, slices all-gathered (NCCL)",
+                           "n": A.n, "nnz": A.nnz, "parallelism": f"column shards x{world}",
+                           "m_equals_whole_build": same, "ms_steps": [round(x, 3) for x in ms]},
+                "gpu_launches": int(launches)}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0 if same else 1
 
 
 def main():
@@ -294,7 +432,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--form", default="m_bf16", choices=list(FORMS))
-    ap.add_argument("--workload", default="cd3d128", choices=["cd3d128", "batch512", "grad512"])
+    ap.add_argument("--workload", default="cd3d128", choices=["cd3d128", "batch512", "grad512", "shard"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-only", action="store_true", help="one plain + one headline solve, no timing loop")
     ap.add_argument("--no-autotune", action="store_true", help="default launch configuration (no dcu_autotune_d)")
@@ -307,6 +445,8 @@ def main():
 
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.workload == "shard":
+        return run_shard(args, rank, world, local)
     if args.workload != "cd3d128":
         return run_extra(args, rank, world)
 

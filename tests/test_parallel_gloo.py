@@ -1,8 +1,9 @@
-"""Column-sharded SPAI build over 2 ranks (gloo, CPU): the split follows the
-reference's distributeColumns and the all-reduce assembles exactly the
-single-process M.  The per-rank column build here is the CPU oracle (there is
-no GPU in this test); on GPUs dcu_b200.parallel.device_slice_builder plugs in
-the library."""
+"""Column-sharded SPAI build over 2 and 3 ranks (gloo, CPU): the split
+follows the reference's distributeColumns and the all-gather of the ranks'
+contiguous slices assembles exactly the single-process M.  The per-rank
+column build here is the CPU oracle (there is no GPU in this test); the
+library's device builder runs the same sharded_build in
+tests/test_gpu_sharded.py."""
 import os
 import socket
 
@@ -33,9 +34,7 @@ def _worker(rank, world, port, schedule, result_path):
 
         def build(start, end):
             m, _, _, _ = oracle.spai(A, "mgs", start, end)
-            full = np.zeros(A.nnz)
-            full[A.ptr[start]:A.ptr[end]] = m[A.ptr[start]:A.ptr[end]]
-            return torch.from_numpy(full)
+            return torch.from_numpy(np.ascontiguousarray(m[A.ptr[start]:A.ptr[end]]))
 
         m = parallel.sharded_build(build, A.ptr, A.n, rank, world, schedule)
         s, e = parallel.column_range(A.ptr, A.n, rank, world, schedule)
@@ -44,8 +43,8 @@ def _worker(rank, world, port, schedule, result_path):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("schedule", [0, 1])
-def test_sharded_build_two_ranks(tmp_path, schedule):
+@pytest.mark.parametrize("world,schedule", [(2, 0), (2, 1), (3, 1)])
+def test_sharded_build_ranks(tmp_path, world, schedule):
     import torch.multiprocessing as mp
 
     import oracle
@@ -53,12 +52,12 @@ def test_sharded_build_two_ranks(tmp_path, schedule):
 
     port = _free_port()
     path = str(tmp_path / "m")
-    mp.start_processes(_worker, args=(2, port, schedule, path), nprocs=2, start_method="spawn", join=True)
+    mp.start_processes(_worker, args=(world, port, schedule, path), nprocs=world, start_method="spawn", join=True)
     A = W.circuit_like()
     full, _, _, _ = oracle.spai(A, "mgs")
-    r0 = np.load(path + ".0.npy")
-    r1 = np.load(path + ".1.npy")
-    # the two ranks cover [0, n) without overlap
-    assert r0[0] == 0 and r0[1] == r1[0] and r1[1] == A.n
-    assert np.array_equal(r0[2:], r1[2:])
-    assert np.array_equal(r0[2:], full)
+    res = [np.load(f"{path}.{r}.npy") for r in range(world)]
+    # the ranks cover [0, n) in order without overlap
+    assert res[0][0] == 0 and res[-1][1] == A.n
+    assert all(res[r][1] == res[r + 1][0] for r in range(world - 1))
+    for r in range(world):
+        assert np.array_equal(res[r][2:], full)
