@@ -90,8 +90,8 @@ def bytes_per_kernel(n, nnz, w_m, w_v, ib, split):
 # command), keyed by (kernel, form).  A constant: ncu does not run inside the
 # benchmark.
 TRAFFIC_BYTES = {
-    ("k_bi_p", "m_bf16"): 50.38e6, ("k_bi_y", "m_bf16"): 49.64e6, ("k_bi_ay", "m_bf16"): 157.94e6,
-    ("k_bi_sz", "m_bf16"): 70.32e6, ("k_bi_az", "m_bf16"): 158.15e6, ("k_bi_xr", "m_bf16"): 110.28e6,
+    ("k_bi_p", "m_bf16"): 50.38e6, ("k_bi_y", "m_bf16"): 52.99e6, ("k_bi_ay", "m_bf16"): 157.94e6,
+    ("k_bi_sz", "m_bf16"): 73.30e6, ("k_bi_az", "m_bf16"): 156.71e6, ("k_bi_xr", "m_bf16"): 110.28e6,
     ("k_bi_py", "fp64"): 178.59e6,
 }
 

@@ -78,7 +78,6 @@ struct SmallArgs {
   const double* val;
   int col_start, col_end;
   int schedule;
-  int units;          // static schedule: balanced_columns split into `units` ranges
   const int* chunks;  // dynamic schedule: nnz-balanced chunk bounds
   int nchunks;
   double* mval;
@@ -424,15 +423,15 @@ __global__ void __launch_bounds__(SG_BLOCK, 12) k_spai_small(SmallArgs a) {
       process(a.list[q]);
     }
   } else if (a.schedule == DCU_SCHED_BALANCED_COLUMNS) {
-    // balanced_columns over `units` contiguous ranges; group q takes units
-    // q, q + ngroups, ...
-    const int total = a.col_end - a.col_start;
-    const int base = total / a.units, rem = total % a.units;
-    for (int u = gid; u < a.units; u += ngroups) {
-      const int start = a.col_start + u * base + min(u, rem);
-      const int end = start + base + (u < rem ? 1 : 0);
-      for (int k = start; k < end; ++k) process(k);
-    }
+    // balanced_columns: the units' contiguous ranges, in order, are the
+    // whole column range; the groups sweep it together, group q taking
+    // columns q, q + ngroups, ...  Equal column counts per group whatever the
+    // unit count, and every group works in one window of the matrix, so a
+    // column's J_k neighbours (up to 16384 columns away in a 3D stencil) are
+    // still in L2 when the neighbouring columns need them.  (Giving each group
+    // its own range spread the groups over the whole matrix: A was read about
+    // twice from DRAM, and a small unit count left most groups idle.)
+    for (int k = a.col_start + gid; k < a.col_end; k += ngroups) process(k);
   } else {
     // nnz-balanced chunks pulled from the queue
     for (;;) {
@@ -473,7 +472,6 @@ struct NeArgs {
   const double* val;
   int col_start, col_end;
   int schedule;
-  int units;
   const int* chunks;
   int nchunks;
   double* mval;
@@ -662,15 +660,9 @@ __global__ void __launch_bounds__(NE_BLOCK) k_spai_ne(NeArgs a) {
   };
 
   if (a.schedule == DCU_SCHED_BALANCED_COLUMNS) {
-    // balanced_columns over `units` ranges; a block takes units b, b + grid, ...
-    // and its threads walk the range together
-    const int total = a.col_end - a.col_start;
-    const int basec = total / a.units, rem = total % a.units;
-    for (int u = blockIdx.x; u < a.units; u += gridDim.x) {
-      const int start = a.col_start + u * basec + min(u, rem);
-      const int end = start + basec + (u < rem ? 1 : 0);
-      for (int k = start + tid; k < end; k += NE_BLOCK) process(k);
-    }
+    // balanced_columns: one sweep of the whole range by all threads (see
+    // k_spai_small)
+    for (int k = a.col_start + blockIdx.x * NE_BLOCK + tid; k < a.col_end; k += gridDim.x * NE_BLOCK) process(k);
   } else {
     for (;;) {
       if (tid == 0) s_chunk = atomicAdd(&a.stats[ST_DYN_HEAD], 1);
@@ -1315,7 +1307,6 @@ int run_small(Ctx* c, SmallArgs a, int) {
   }
   const int grid = c->sms * per_sm;
   const int ngroups = grid * SG_BLOCK / GL;
-  if (a.units <= 0) a.units = ngroups;
   if (a.schedule == DCU_SCHED_BALANCED_NNZ) {
     const int nchunks = ngroups * 4;
     DCU_TRY(ensure(c, B_CHUNKS, sizeof(int) * (size_t)(nchunks + 1)));
@@ -1430,7 +1421,6 @@ int run_ne(Ctx* c, NeArgs a) {
     per_sm = 1;
   }
   const int grid = c->sms * per_sm;
-  if (a.units <= 0) a.units = grid;
   if (a.schedule == DCU_SCHED_BALANCED_NNZ) {
     const int nchunks = grid * 8;
     DCU_TRY(ensure(c, B_CHUNKS, sizeof(int) * (size_t)(nchunks + 1)));
@@ -1470,7 +1460,6 @@ int prepare(Ctx* c, int n, const int* ptr, const int* idx, const double* val, in
   a.schedule = schedule;
   a.big_list = bp<int>(c, B_BIGLIST);
   a.stats = stats;
-  a.units = c->units;
   a.max_ni = SG_MMAX;
   P->stats = stats;
   return DCU_OK;
@@ -1505,7 +1494,6 @@ int build_typed(Ctx* c, int n, const int* ptr, const int* idx, const double* val
     na.col_start = col_start;
     na.col_end = col_end;
     na.schedule = schedule;
-    na.units = c->units_user ? c->units : 0;
     na.mval = mval;
     na.colres = colres;
     na.fb_list = bp<int>(c, B_FBLIST);

@@ -148,9 +148,13 @@ void dcu_options_default(dcu_options* opt);
 /* ---- context ------------------------------------------------------------- */
 
 /* Create a context on CUDA device `device`.  `units` is the schedule's unit
- * count P (the reference's numDCUs): balanced_columns splits the columns into
- * P contiguous ranges that the resident warps take in turn; <= 0 picks one
- * unit per resident warp of the column kernel.  Replaces initMultiDCU. */
+ * count P (the reference's numDCUs; <= 0 picks one per resident warp group of
+ * the column kernel): the P contiguous ranges of balanced_columns that
+ * dcu_spai_distribute_columns reports and the sharded build uses.  On one
+ * device the static schedule takes those ranges in order, which is the whole
+ * column range, in one sweep by all resident workers (equal column counts per
+ * worker for any P); the dynamic schedule pulls nnz-balanced chunks from an
+ * atomic queue.  M does not depend on either.  Replaces initMultiDCU. */
 int dcu_spai_create(dcu_spai_ctx** ctx, int device, int units);
 /* Frees every device buffer the context owns.  Replaces cleanupMultiDCU. */
 void dcu_spai_destroy(dcu_spai_ctx* ctx);

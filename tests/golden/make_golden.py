@@ -73,6 +73,18 @@ def fixture(path):
     r = oracle.bicgstab(A, m, b, None, tol=1e-8, tol_mode="rel", maxiter=1000)
     out["config_settings"] = {"iters": r["iters"], "status": r["status"],
                               "rel_res": r["true_res"] / float(np.linalg.norm(b))}
+    if oracle.emu_available():
+        # the same through the reference's own code: its SPAI kernels on the
+        # host SIMT emulator, its BiCGSTAB over the host library stand-ins
+        # (the config setting as its absolute threshold 1e-8 ||b|| with x0 = 0)
+        me, info = oracle.refemu_spai(A)
+        rr = oracle.refemu_bicgstab(A, me, np.ones(A.n), np.ones(A.n), 1e-7, 10000)
+        rc = oracle.refemu_bicgstab(A, me, b, np.zeros(A.n), 1e-8 * float(np.linalg.norm(b)), 1000)
+        out["reference_code"] = {
+            "m_rel_diff_vs_oracle": float(np.max(np.abs(me - m)) / np.max(np.abs(m))),
+            "single_pass": bool(info[3]), "tiles": int(info[2]), "n1max": int(info[0]), "n2max": int(info[1]),
+            "reference_settings_iters": rr["iters"], "config_settings_iters": rc["iters"],
+            "config_settings_rel_res": float(np.linalg.norm(b - A.matvec(rc["x"])) / np.linalg.norm(b))}
     return out
 
 

@@ -206,3 +206,30 @@ def test_hub_column_with_fewer_rows_than_columns(ctx):
     for k in range(1, A.n):
         a, b = m[A.ptr[k]:A.ptr[k + 1]], m_h[A.ptr[k]:A.ptr[k + 1]]
         assert np.max(np.abs(a - b)) <= RTOL_FP64 * max(1.0, np.max(np.abs(b))), k
+
+
+def test_static_schedule_speed_does_not_depend_on_units():
+    """balanced_columns with one unit (one "DCU") must not serialise the build:
+    the resident workers sweep the units' ranges together.  (Giving each
+    worker its own unit once left all but one worker idle: ~3400x slower at
+    128^3 with one unit.)  The bound is loose; the columns are identical."""
+    import torch
+
+    from dcu_b200.api import Context
+
+    A = W.convdiff3d(48, 20.0)
+    d = lambda x: torch.from_numpy(np.ascontiguousarray(x)).cuda()
+    p, i, v = d(A.ptr), d(A.idx), d(A.val)
+    out = {}
+    for units in (0, 1, 3):
+        with Context(0, units=units) as c:
+            for prec in (N.PREC_FP64, N.PREC_M_BF16):
+                m = torch.zeros(A.nnz, dtype=torch.float64, device="cuda")
+                ms = min(c.build_d(A.n, A.nnz, p, i, v, m, precision=prec).ms for _ in range(3))
+                out[(units, prec)] = (ms, m.cpu().numpy())
+    for prec in (N.PREC_FP64, N.PREC_M_BF16):
+        base_ms, base_m = out[(0, prec)]
+        for units in (1, 3):
+            ms, m = out[(units, prec)]
+            assert np.array_equal(m, base_m)
+            assert ms < 5.0 * base_ms + 0.2, (units, prec, ms, base_ms)
