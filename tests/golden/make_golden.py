@@ -146,6 +146,26 @@ def batch_sensitivity(trials=4, systems=64):
             "trials": trials}
 
 
+def fixture_sensitivity(trials=8):
+    """The same spread on the reference's circuit_2 fixture, in the reference's
+    solver settings and in the configs' (M from the Householder oracle)."""
+    path = oracle.fixture_path("circuit_2.mtx")
+    A = oracle.ref_mtx_read(path)
+    m, _, _, _ = oracle.spai(A, "householder")
+    one = np.ones(A.n)
+    b = W.rhs_ones_product(A)
+    runs = {"reference_settings": lambda mm: oracle.bicgstab(A, mm, one, one, tol=1e-7, tol_mode="abs",
+                                                             maxiter=10000)["iters"],
+            "config_settings": lambda mm: oracle.bicgstab(A, mm, b, None, tol=1e-8, tol_mode="rel",
+                                                          maxiter=1000)["iters"]}
+    out = {"trials": trials}
+    for key, run in runs.items():
+        base = run(m)
+        its = [run(_perturbed(m, t)) for t in range(1, trials + 1)]
+        out[key] = {"iters": base, "perturbed": its, "iters_band": max(1, max(abs(v - base) for v in its))}
+    return out
+
+
 def sensitivity(trials=8):
     """Spread of the oracle's own BiCGSTAB iteration count when M moves by one
     ulp per value, on the benchmark workloads with long solves: the band a
@@ -188,6 +208,12 @@ def sensitivity(trials=8):
 if __name__ == "__main__":
     if "--sensitivity" in sys.argv:
         sensitivity()
+    elif "--fixture-sensitivity" in sys.argv:
+        path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "sensitivity.json")
+        out = json.load(open(path))
+        out["circuit_2_mtx"] = fixture_sensitivity()
+        with open(path, "w") as f:
+            json.dump(out, f, indent=1, sort_keys=True)
     elif "--batch-sensitivity" in sys.argv:
         path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "sensitivity.json")
         out = json.load(open(path))

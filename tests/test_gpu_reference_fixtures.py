@@ -7,9 +7,12 @@ SHA-256), through the C ABI and both command-line drivers.
 circuit_2 exercises the hub path: |J| up to 1285 and |I| up to 4510 (every
 row), blocks far beyond one CTA's shared memory.  Expected values are the
 oracle's (tests/golden/golden.json, "fixtures"): M within 1e-10 of the
-Householder oracle (which matches the MGS oracle to 5e-13 on every column),
-BiCGSTAB iterations within one of the oracle's in the reference's solver
-settings and in the configs'.  fill_3elt does not converge in either setting.
+Householder oracle (which matches the MGS oracle to 5e-13 on every column and
+the reference's own kernels to 2e-16), BiCGSTAB iterations within the spread
+the count shows under rounding-level changes of M: the larger of the oracle's
+own one-ulp spread (tests/golden/sensitivity.json: 71-74 around 74 in the
+reference's settings, 58-60 around 58 in the configs') and the distance to
+the reference's own code run on its own M (74 and 61).  fill_3elt does not converge in either setting.
 Its iterates wander without converging, and whether a recurrence scalar
 (rho, (r*, A y)) comes out exactly zero on the way depends on the summation
 order: the oracle and the reference's own BiCGSTAB code over the stand-in
@@ -19,6 +22,7 @@ MAX_ITER; here the solver stops with the breakdown status.  So the GPU must end
 unconverged with either status, and the reference-compatible count (the
 legacy entry point, through the driver) is MAX_ITER either way."""
 import hashlib
+import json
 import os
 import re
 import subprocess
@@ -35,6 +39,17 @@ from tests.test_golden import GOLDEN, digest
 pytestmark = pytest.mark.gpu
 
 FIX = GOLDEN.get("fixtures", {})
+SENS = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "sensitivity.json")))
+
+
+def _band(name, setting):
+    """Iteration band of a fixture and solver setting (see the module docstring)."""
+    g = FIX[name]
+    band = SENS.get(name.replace(".", "_"), {}).get(setting, {}).get("iters_band", 1)
+    rc = g.get("reference_code")
+    if rc:
+        band = max(band, abs(rc[setting + "_iters"] - g[setting]["iters"]))
+    return band
 
 
 def _load(name):
@@ -81,14 +96,14 @@ def test_circuit2_spai_and_solves(ctx, schedule):
     x, si = ctx.bicgstab_h(A, m, np.ones(A.n), np.ones(A.n), tol=1e-7, tol_mode=N.TOL_ABS, maxiter=10000,
                            verify=0)
     assert si.status == N.SOLVE_CONVERGED and rs["status"] == 0
-    assert abs(si.iters - rs["iters"]) <= 1, (si.iters, rs["iters"])
+    assert abs(si.iters - rs["iters"]) <= _band("circuit_2.mtx", "reference_settings"), (si.iters, rs["iters"])
     assert np.linalg.norm(np.ones(A.n) - A.matvec(x)) < 1e-6
     # the configs' settings
     cs = g["config_settings"]
     b = W.rhs_ones_product(A)
     x, _, bi, si = ctx.solve_h(A, b)
     assert si.status == N.SOLVE_CONVERGED and cs["status"] == 0
-    assert abs(si.iters - cs["iters"]) <= 1, (si.iters, cs["iters"])
+    assert abs(si.iters - cs["iters"]) <= _band("circuit_2.mtx", "config_settings"), (si.iters, cs["iters"])
     assert np.linalg.norm(b - A.matvec(x)) / np.linalg.norm(b) < 1e-8
 
 
@@ -144,7 +159,8 @@ def test_multi_driver_default_input(algo):
     m = re.search(r"^\[ALGO_REPORT\] mode=(\w+), dcu_units=(\d+), partition=(\w+), preconditioner_ms=([0-9.]+), "
                   r"iteration_count=(\d+)$", out.stdout, re.M)
     assert m, out.stdout
-    assert abs(int(m.group(5)) - FIX["circuit_2.mtx"]["reference_settings"]["iters"]) <= 1
+    assert abs(int(m.group(5)) - FIX["circuit_2.mtx"]["reference_settings"]["iters"]) <= _band(
+        "circuit_2.mtx", "reference_settings")
 
 
 def test_single_driver_default_input():
@@ -153,7 +169,8 @@ def test_single_driver_default_input():
     assert out.returncode == 0, out.stderr
     it = re.search(r"^ ?iter_times = (\d+), err/err0=\s*([0-9.eE+-]+) $", out.stdout, re.M)
     assert it, out.stdout
-    assert abs(int(it.group(1)) - FIX["circuit_2.mtx"]["reference_settings"]["iters"]) <= 1
+    assert abs(int(it.group(1)) - FIX["circuit_2.mtx"]["reference_settings"]["iters"]) <= _band(
+        "circuit_2.mtx", "reference_settings")
     assert float(it.group(2)) < 1e-7
     times = {}
     for key in ("preconditioningTime", "solvingTime", "totalTime"):
