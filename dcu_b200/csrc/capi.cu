@@ -55,15 +55,20 @@ int resolve_range(Ctx* c, int n, const dcu_options* in, dcu_options* out) {
   return DCU_OK;
 }
 
-// A's values (FP64) and M's (by form) in SELL order; an FP32 / BF16 M's
-// narrow slices row-major in *msell8 (NULL for an FP64 M).
-int gather_values(Ctx* c, const dcu::SellPlan& pl, const double* val, const double* mval, int precision,
-                  const void** msell, const void** msell8) {
+// A's values (FP64) in SELL order.
+int gather_a(Ctx* c, const dcu::SellPlan& plan, const double* val) {
+  const size_t slots = (size_t)(plan.slots > 0 ? plan.slots : 1);
+  DCU_TRY(dcu::ensure(c, dcu::B_SELL_AVAL, sizeof(double) * slots));
+  return dcu::sell_gather_f64(c, plan, val, dcu::bp<double>(c, dcu::B_SELL_AVAL));
+}
+
+// M's values (by form) in SELL order; an FP32 / BF16 M's narrow slices
+// row-major in *msell8 (NULL for an FP64 M).
+int gather_m(Ctx* c, const dcu::SellPlan& pl, const double* mval, int precision, const void** msell,
+             const void** msell8) {
   const dcu::SellPlan* plan = &pl;
   const size_t slots = (size_t)(plan->slots > 0 ? plan->slots : 1);
   const size_t rows8 = (size_t)plan->nslices * 32 * dcu::kNarrow;
-  DCU_TRY(dcu::ensure(c, dcu::B_SELL_AVAL, sizeof(double) * slots));
-  DCU_TRY(dcu::sell_gather_f64(c, *plan, val, dcu::bp<double>(c, dcu::B_SELL_AVAL)));
   if (precision == DCU_PREC_FP64) {
     DCU_TRY(dcu::ensure(c, dcu::B_SELL_MVAL, sizeof(double) * slots));
     DCU_TRY(dcu::sell_gather_f64(c, *plan, mval, dcu::bp<double>(c, dcu::B_SELL_MVAL)));
@@ -82,6 +87,22 @@ int gather_values(Ctx* c, const dcu::SellPlan& pl, const double* val, const doub
   *msell8 = precision == DCU_PREC_FP64 ? nullptr : c->buf[dcu::B_SELL_MVAL8].p;
   return DCU_OK;
 }
+
+// A's values (FP64) and M's (by form) in SELL order.
+int gather_values(Ctx* c, const dcu::SellPlan& plan, const double* val, const double* mval, int precision,
+                  const void** msell, const void** msell8) {
+  DCU_TRY(gather_a(c, plan, val));
+  return gather_m(c, plan, mval, precision, msell, msell8);
+}
+
+// Points the context's stream at `s` for a scope (the plan and gather
+// helpers enqueue on c->stream and synchronise it).
+struct OnStream {
+  Ctx* c;
+  cudaStream_t saved;
+  OnStream(Ctx* ctx, cudaStream_t s) : c(ctx), saved(ctx->stream) { c->stream = s; }
+  ~OnStream() { c->stream = saved; }
+};
 
 // Solver-side layout of A and M: SELL plan + values.
 int prepare_solve(Ctx* c, int n, int nnz, const int* ptr, const int* idx, const double* val, const double* mval,
@@ -104,17 +125,31 @@ int solve_pipeline(Ctx* c, int n, int nnz, const int* ptr, const int* idx, const
     m = dcu::bp<double>(c, dcu::B_MVAL);
   }
   DCU_TRY(dcu::validate_csc(c, n, nnz, ptr, idx));
-  dcu::SellPlan plan;
-  DCU_TRY(dcu::sell_plan(c, n, nnz, ptr, idx, &plan));
+  DCU_CUDA(c, cudaEventRecord(c->ev[6], c->stream));
   if (val_ready) DCU_CUDA(c, cudaStreamWaitEvent(c->stream, val_ready, 0));
   dcu_build_info bl{};
   // the build's time is read after the solve's final synchronisation: no
   // host round trip between the build and the solver's first launches
   DCU_CUDA(c, cudaEventRecord(c->ev[4], c->stream));
-  DCU_TRY(dcu::spai_build(c, n, nnz, ptr, idx, val, &o, m, nullptr, &bl));
+  dcu::BuildJob job;
+  DCU_TRY(dcu::spai_build_launch(c, n, nnz, ptr, idx, val, &o, m, nullptr, &job));
+  // While the build's first kernel runs: the SELL plan (pattern only) and A's
+  // values in SELL order on the auxiliary stream, whose host round trips wait
+  // for that stream alone.
+  dcu::SellPlan plan;
+  {
+    OnStream aux(c, c->aux_stream);
+    DCU_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev[6], 0));
+    DCU_TRY(dcu::sell_plan(c, n, nnz, ptr, idx, &plan));
+    if (val_ready) DCU_CUDA(c, cudaStreamWaitEvent(c->stream, val_ready, 0));
+    DCU_TRY(gather_a(c, plan, val));
+    DCU_CUDA(c, cudaEventRecord(c->ev[7], c->stream));
+  }
+  DCU_TRY(dcu::spai_build_finish(c, &job, &bl));
   DCU_CUDA(c, cudaEventRecord(c->ev[5], c->stream));
+  DCU_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev[7], 0));
   const void *msell = nullptr, *msell8 = nullptr;
-  DCU_TRY(gather_values(c, plan, val, m, o.precision, &msell, &msell8));
+  DCU_TRY(gather_m(c, plan, m, o.precision, &msell, &msell8));
   if (bx_ready) DCU_CUDA(c, cudaStreamWaitEvent(c->stream, bx_ready, 0));
   DCU_TRY(dcu::bicgstab_solve(c, plan, dcu::bp<double>(c, dcu::B_SELL_AVAL), msell, b, x, &o, sinfo, msell8));
   DCU_CUDA(c, cudaEventSynchronize(c->ev[5]));
@@ -422,8 +457,9 @@ int dcu_spai_create(dcu_spai_ctx** out, int device, int units) {
     if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) { rc = dcu::cuda_fail(c, e, "stream", __FILE__, __LINE__); break; }
     if ((e = cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking)) != cudaSuccess) { rc = dcu::cuda_fail(c, e, "copy stream", __FILE__, __LINE__); break; }
     if ((e = cudaMallocHost(&c->pinned, dcu::kPinnedBytes)) != cudaSuccess) { rc = dcu::cuda_fail(c, e, "cudaMallocHost", __FILE__, __LINE__); break; }
-    for (int i = 0; i < 6 && e == cudaSuccess; ++i)
-      e = cudaEventCreateWithFlags(&c->ev[i], (i < 2 || i >= 4) ? cudaEventDefault : cudaEventDisableTiming);
+    if ((e = cudaStreamCreateWithFlags(&c->aux_stream, cudaStreamNonBlocking)) != cudaSuccess) { rc = dcu::cuda_fail(c, e, "aux stream", __FILE__, __LINE__); break; }
+    for (int i = 0; i < 8 && e == cudaSuccess; ++i)
+      e = cudaEventCreateWithFlags(&c->ev[i], (i < 2 || i == 4 || i == 5) ? cudaEventDefault : cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_sync, cudaEventDisableTiming);
     if (e != cudaSuccess) { rc = dcu::cuda_fail(c, e, "events", __FILE__, __LINE__); break; }
   } while (0);
@@ -444,6 +480,7 @@ void dcu_spai_destroy(dcu_spai_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
+  if (c->aux_stream) cudaStreamSynchronize(c->aux_stream);
   dcu::release_graphs(c);
   for (auto& b : c->buf)
     if (b.p) cudaFree(b.p);
@@ -453,6 +490,7 @@ void dcu_spai_destroy(dcu_spai_ctx* c) {
   if (c->pinned) cudaFreeHost(c->pinned);
   if (c->stream) cudaStreamDestroy(c->stream);
   if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+  if (c->aux_stream) cudaStreamDestroy(c->aux_stream);
   delete c;
 }
 

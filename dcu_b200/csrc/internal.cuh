@@ -90,6 +90,7 @@ struct Ctx {
   size_t smem_optin = 0;
   cudaStream_t stream = nullptr;       // the context's own non-blocking stream
   cudaStream_t copy_stream = nullptr;  // host-API uploads that overlap work on `stream`
+  cudaStream_t aux_stream = nullptr;   // a whole solve's SELL plan and A gather, beside the build
   cudaStream_t user_stream = nullptr;  // caller's stream to order against (optional)
   cudaEvent_t ev_sync = nullptr;       // ordering between user_stream and stream
   std::string err;
@@ -98,8 +99,9 @@ struct Ctx {
   void* pinned = nullptr;   // small pinned host scratch (flags, stats), kPinnedBytes
   // ev[0..1]: timing of one call's device work; ev[2..3]: the solver's
   // stop-flag polling; ev[4..5]: the build inside a whole solve, read only
-  // after the solve's own final synchronisation
-  cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  // after the solve's own final synchronisation; ev[6..7]: ordering of the
+  // auxiliary stream (start after validation, join before M's gather)
+  cudaEvent_t ev[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   std::vector<GraphSlot> graphs;  // BiCGSTAB iteration graphs (bounded cache)
   // launch configuration per precision form (dcu_set_tuning / dcu_autotune_d)
   dcu_tuning tune[5];
@@ -233,6 +235,32 @@ int sell_gather_m8_bf16(Ctx* c, const SellPlan& p, const double* src, __nv_bfloa
 // ---------------------------------------------------------------------------
 // SPAI build and pattern.
 // ---------------------------------------------------------------------------
+// A SPAI build split in two (spai_build = launch + finish): the launch
+// enqueues the first column kernel on c->stream and returns without waiting;
+// the finish completes the build (host round trips, further kernels) and
+// fills info.  Work on other streams may run between the two.
+struct BuildJobImpl;  // the prepared launch arguments (spai_build.cu)
+struct BuildJob {
+  dcu_options opt{};
+  int n = 0;
+  const int* ptr = nullptr;
+  const int* idx = nullptr;
+  const double* val = nullptr;
+  double* mval = nullptr;
+  double* colres = nullptr;
+  bool empty = false;
+  bool thread_path = false;
+  int max_ni = 0, cta_max_area = 0;
+  int* fb_list = nullptr;
+  BuildJobImpl* impl;
+  BuildJob();
+  ~BuildJob();
+  BuildJob(const BuildJob&) = delete;
+  BuildJob& operator=(const BuildJob&) = delete;
+};
+int spai_build_launch(Ctx* c, int n, int nnz, const int* ptr, const int* idx, const double* val,
+                      const dcu_options* opt, double* mval, double* colres, BuildJob* job);
+int spai_build_finish(Ctx* c, BuildJob* job, dcu_build_info* info);
 int spai_build(Ctx* c, int n, int nnz, const int* ptr, const int* idx, const double* val,
                const dcu_options* opt, double* mval, double* colres, dcu_build_info* info);
 // Work units of the static schedule when the caller names none: one per

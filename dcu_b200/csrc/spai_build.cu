@@ -1441,6 +1441,14 @@ struct Prepared {
   int* stats = nullptr;
 };
 
+}  // namespace
+
+struct BuildJobImpl {
+  Prepared P;
+};
+
+namespace {
+
 int prepare(Ctx* c, int n, const int* ptr, const int* idx, const double* val, int col_start, int col_end,
             int schedule, Prepared* P) {
   const int ncols = col_end - col_start;
@@ -1473,16 +1481,20 @@ int read_stats(Ctx* c, int* host) {
   return DCU_OK;
 }
 
+// A build in two halves: the launch enqueues the first column kernel and
+// returns without waiting; the finish reads its statistics (a host round
+// trip), runs the hand-offs, the CTA kernel and the hub kernels, and fills
+// info.  Between the two the caller may enqueue independent work on other
+// streams (the solver's SELL plan), which then overlaps the first kernel.
 template <typename T>
-int build_typed(Ctx* c, int n, const int* ptr, const int* idx, const double* val, int col_start, int col_end,
-                int schedule, bool thread_path, int max_ni, int cta_max_area, double* mval, double* colres,
-                dcu_build_info* info) {
-  Prepared P;
+int build_launch(Ctx* c, int n, const int* ptr, const int* idx, const double* val, int col_start, int col_end,
+                 int schedule, bool thread_path, int max_ni, double* mval, double* colres, BuildJob* J) {
+  Prepared& P = J->impl->P;
   DCU_TRY(prepare(c, n, ptr, idx, val, col_start, col_end, schedule, &P));
   if (max_ni > 0 && max_ni < SG_MMAX) P.sa.max_ni = max_ni;
   P.sa.mval = mval;
   P.sa.colres = colres;
-  int st[ST_INTS];
+  J->thread_path = thread_path;
   if (thread_path) {
     // thread per column first; its hand-offs go to the group kernel
     DCU_TRY(ensure(c, B_FBLIST, sizeof(int) * (size_t)(col_end - col_start)));
@@ -1499,14 +1511,25 @@ int build_typed(Ctx* c, int n, const int* ptr, const int* idx, const double* val
     na.fb_list = bp<int>(c, B_FBLIST);
     na.stats = P.stats;
     na.tau = sizeof(T) == sizeof(float) ? 1e-3 : 1e-8;
+    J->fb_list = na.fb_list;
     DCU_TRY(run_ne<T>(c, na));
-    DCU_TRY(read_stats(c, st));
-    if (st[ST_FB_COUNT] > 0) {
-      P.sa.list = na.fb_list;
-      DCU_TRY((run_small<T, MODE_BUILD>(c, P.sa, P.grid)));
-    }
   } else {
     DCU_TRY((run_small<T, MODE_BUILD>(c, P.sa, P.grid)));
+  }
+  return DCU_OK;
+}
+
+template <typename T>
+int build_finish(Ctx* c, int n, const int* ptr, const int* idx, const double* val, int col_start, int col_end,
+                 int cta_max_area, double* mval, double* colres, BuildJob* J, dcu_build_info* info) {
+  Prepared& P = J->impl->P;
+  int st[ST_INTS];
+  if (J->thread_path) {
+    DCU_TRY(read_stats(c, st));
+    if (st[ST_FB_COUNT] > 0) {
+      P.sa.list = J->fb_list;
+      DCU_TRY((run_small<T, MODE_BUILD>(c, P.sa, P.grid)));
+    }
   }
   DCU_TRY(read_stats(c, st));
   const int nbig = st[ST_BIG_COUNT];
@@ -1558,25 +1581,56 @@ int spai_default_units(Ctx* c) {
   return c->sms * per_sm * (SG_BLOCK / GL);
 }
 
-int spai_build(Ctx* c, int n, int nnz, const int* ptr, const int* idx, const double* val, const dcu_options* opt,
-               double* mval, double* colres, dcu_build_info* info) {
+BuildJob::BuildJob() : impl(new BuildJobImpl) {}
+BuildJob::~BuildJob() { delete impl; }
+
+int spai_build_launch(Ctx* c, int n, int nnz, const int* ptr, const int* idx, const double* val,
+                      const dcu_options* opt, double* mval, double* colres, BuildJob* J) {
   const int col_start = opt->col_start;
   const int col_end = opt->col_end;
+  J->opt = *opt;
+  J->n = n;
+  J->ptr = ptr;
+  J->idx = idx;
+  J->val = val;
+  J->mval = mval;
+  J->colres = colres;
+  J->empty = false;
   if (col_start != 0 || col_end != n)
     DCU_CUDA(c, cudaMemsetAsync(mval, 0, sizeof(double) * (size_t)(nnz > 0 ? nnz : 1), c->stream));
-  if (col_end <= col_start) return DCU_OK;
+  if (col_end <= col_start) {
+    J->empty = true;
+    return DCU_OK;
+  }
   const int p = opt->precision;
   const bool tuned = p >= 0 && p < 5 && c->tune_set[p];
-  const int max_ni = tuned ? c->tune[p].group_max_ni : 0;
-  const int cta_max_area = tuned ? c->tune[p].cta_max_area : 0;
+  J->max_ni = tuned ? c->tune[p].group_max_ni : 0;
+  J->cta_max_area = tuned ? c->tune[p].cta_max_area : 0;
   // FP64 (the plain form): Householder on every column unless the normal
   // equations are asked for.  Mixed forms: the thread-per-column path first,
   // Householder for the columns it hands over, unless Householder is asked for.
   if (opt->precision == DCU_PREC_FP64)
-    return build_typed<double>(c, n, ptr, idx, val, col_start, col_end, opt->schedule,
-                               opt->ls_method == DCU_LS_NORMAL_EQ, max_ni, cta_max_area, mval, colres, info);
-  return build_typed<float>(c, n, ptr, idx, val, col_start, col_end, opt->schedule, opt->ls_method != DCU_LS_HOUSEHOLDER,
-                            max_ni, cta_max_area, mval, colres, info);
+    return build_launch<double>(c, n, ptr, idx, val, col_start, col_end, opt->schedule,
+                                opt->ls_method == DCU_LS_NORMAL_EQ, J->max_ni, mval, colres, J);
+  return build_launch<float>(c, n, ptr, idx, val, col_start, col_end, opt->schedule,
+                             opt->ls_method != DCU_LS_HOUSEHOLDER, J->max_ni, mval, colres, J);
+}
+
+int spai_build_finish(Ctx* c, BuildJob* J, dcu_build_info* info) {
+  if (J->empty) return DCU_OK;
+  const dcu_options& o = J->opt;
+  if (o.precision == DCU_PREC_FP64)
+    return build_finish<double>(c, J->n, J->ptr, J->idx, J->val, o.col_start, o.col_end, J->cta_max_area,
+                                J->mval, J->colres, J, info);
+  return build_finish<float>(c, J->n, J->ptr, J->idx, J->val, o.col_start, o.col_end, J->cta_max_area, J->mval,
+                             J->colres, J, info);
+}
+
+int spai_build(Ctx* c, int n, int nnz, const int* ptr, const int* idx, const double* val, const dcu_options* opt,
+               double* mval, double* colres, dcu_build_info* info) {
+  BuildJob J;
+  DCU_TRY(spai_build_launch(c, n, nnz, ptr, idx, val, opt, mval, colres, &J));
+  return spai_build_finish(c, &J, info);
 }
 
 int spai_pattern(Ctx* c, int n, const int* ptr, const int* idx, int col_start, int col_end, int* icount,
