@@ -133,6 +133,8 @@ int solve_pipeline(Ctx* c, int n, int nnz, const int* ptr, const int* idx, const
   DCU_CUDA(c, cudaEventRecord(c->ev[4], c->stream));
   dcu::BuildJob job;
   DCU_TRY(dcu::spai_build_launch(c, n, nnz, ptr, idx, val, &o, m, nullptr, &job));
+  // the build's end: after its first kernel, unless the finish adds kernels
+  DCU_CUDA(c, cudaEventRecord(c->ev[5], c->stream));
   // While the build's first kernel runs: the SELL plan (pattern only) and A's
   // values in SELL order on the auxiliary stream, whose host round trips wait
   // for that stream alone.
@@ -146,7 +148,7 @@ int solve_pipeline(Ctx* c, int n, int nnz, const int* ptr, const int* idx, const
     DCU_CUDA(c, cudaEventRecord(c->ev[7], c->stream));
   }
   DCU_TRY(dcu::spai_build_finish(c, &job, &bl));
-  DCU_CUDA(c, cudaEventRecord(c->ev[5], c->stream));
+  if (job.finish_launched) DCU_CUDA(c, cudaEventRecord(c->ev[5], c->stream));
   DCU_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev[7], 0));
   const void *msell = nullptr, *msell8 = nullptr;
   DCU_TRY(gather_m(c, plan, m, o.precision, &msell, &msell8));

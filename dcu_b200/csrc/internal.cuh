@@ -252,6 +252,7 @@ struct BuildJob {
   bool thread_path = false;
   int max_ni = 0, cta_max_area = 0;
   int* fb_list = nullptr;
+  bool finish_launched = false;  // the finish enqueued kernels of its own
   BuildJobImpl* impl;
   BuildJob();
   ~BuildJob();

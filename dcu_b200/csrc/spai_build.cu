@@ -1528,6 +1528,7 @@ int build_finish(Ctx* c, int n, const int* ptr, const int* idx, const double* va
     DCU_TRY(read_stats(c, st));
     if (st[ST_FB_COUNT] > 0) {
       P.sa.list = J->fb_list;
+      J->finish_launched = true;
       DCU_TRY((run_small<T, MODE_BUILD>(c, P.sa, P.grid)));
     }
   }
@@ -1550,6 +1551,7 @@ int build_finish(Ctx* c, int n, const int* ptr, const int* idx, const double* va
     memcpy(&area, reinterpret_cast<long long*>(st) + ST_AREA64, sizeof area);
     la.area_per_block = area;
     memcpy(&la.area_sum, reinterpret_cast<long long*>(st) + ST_AREASUM64, sizeof la.area_sum);
+    J->finish_launched = true;
     DCU_TRY((run_large<T, MODE_BUILD>(c, la, nbig, cta_max_area)));
     DCU_TRY(read_stats(c, st));
     if (st[ST_LIMIT] > 0) return fail(c, DCU_ERR_LIMIT, "%d columns exceeded the CTA kernel's limits", st[ST_LIMIT]);
