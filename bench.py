@@ -68,18 +68,19 @@ def index_bytes(n, w_i, slots, uniform_slots):
     return w_i * (slots - uniform_slots) + 4 * (uniform_slots // 32) + 12 * ((n + 31) // 32)
 
 
-def bytes_per_kernel(n, nnz, w_m, w_v, ib, split):
+def bytes_per_kernel(n, nnz, w_m, w_v, ib, split, w_a=8):
     """Algorithmic HBM bytes of each iteration kernel (one launch), in the
-    order of iteration_kernels(split); ib = index_bytes() of one SpMV."""
+    order of iteration_kernels(split); ib = index_bytes() of one SpMV; w_a =
+    bytes of an A value read (4 when the solve reads A's exact FP32 copy)."""
     if split:
         k1 = [n * (16 + 2 * w_v),                           # K1a p = r + beta(p - w ay)
               nnz * w_m + ib + n * 2 * w_v]                 # K1b y = M p
     else:
         k1 = [nnz * w_m + ib + n * (16 + 3 * w_v)]         # K1 p on the fly, y = M p
     return k1 + [
-        nnz * 8 + ib + n * (8 + 2 * w_v),         # K2 ay = A y, (r*, ay)
+        nnz * w_a + ib + n * (8 + 2 * w_v),       # K2 ay = A y, (r*, ay)
         nnz * w_m + ib + n * (24 + w_v),          # K3 s = r - alpha ay, z = M s
-        nnz * 8 + ib + n * (16 + w_v),            # K4 az = A z, (az, s), (az, az)
+        nnz * w_a + ib + n * (16 + w_v),          # K4 az = A z, (az, s), (az, az)
         n * (40 + 3 * w_v),                       # K5 x, r update, (r*, r), (r, r)
     ]
 
@@ -528,7 +529,16 @@ def main():
                 solve(f)
             msf, inff, _ = timed(f, steps)
             forms[name] = {"ms": round(statistics.mean(msf), 3), "iters": inff[-1][1].iters,
-                           "build_ms": round(inff[-1][0].ms, 3)}
+                           "build_ms": round(inff[-1][0].ms, 3), "a_fp32": inff[-1][1].a_fp32}
+        # the headline form with A read from its FP64 array (the same numbers:
+        # bit-identical iterates; what the exact FP32 copy saves)
+        ctx.set_exact_a32(False)
+        for _ in range(2):
+            solve(head)
+        msf, inff, _ = timed(head, steps)
+        forms[args.form + "_a_fp64_reads"] = {"ms": round(statistics.mean(msf), 3), "iters": inff[-1][1].iters,
+                                              "a_fp32": inff[-1][1].a_fp32}
+        ctx.set_exact_a32(True)
         barrier()
 
     relres_plain = float(np.linalg.norm(b_h - A.matvec(x_plain)) / np.linalg.norm(b_h))
@@ -542,7 +552,8 @@ def main():
     split = len(kms) == 6
     w_m, w_v, w_i = form_widths(head)
     slots, uslots = ctx.sell_plan_stats()
-    kbytes = bytes_per_kernel(n, nnz, w_m, w_v, index_bytes(n, w_i, slots, uslots), split)
+    w_a = 4 if inf_head[-1][1].a_fp32 else 8
+    kbytes = bytes_per_kernel(n, nnz, w_m, w_v, index_bytes(n, w_i, slots, uslots), split, w_a)
     j = int(np.argmax(kms))
     peaks = {}
     try:
@@ -571,8 +582,9 @@ def main():
     # iterations x iteration bytes, over the timed ms
     # (with the fused first step's bytes, the fewer of the two, whichever
     # step the autotuner picked)
-    pbytes = sum(bytes_per_kernel(n, nnz, 8, 8, index_bytes(n, 4, slots, uslots), False))
     pl_last = inf_plain[-1]
+    pbytes = sum(bytes_per_kernel(n, nnz, 8, 8, index_bytes(n, 4, slots, uslots), False,
+                                  4 if pl_last[1].a_fp32 else 8))
     p_us = pl_last[1].ms * 1e3 / max(1, pl_last[1].iters)
     p_gbs = pbytes / (p_us * 1e-6) / 1e9
     roofline["plain_iteration"] = {"bytes": int(pbytes), "us": round(p_us, 1), "achieved": round(p_gbs, 1),
@@ -690,6 +702,8 @@ def main():
                        "parallelism": f"replicas x{world}" if world > 1 else "single",
                        "l2": "flushed between steps (256 MB write); A alone is 175 MB > L2",
                        "iters": hi_[1].iters, "build_ms": round(hi_[0].ms, 3), "solve_ms": round(hi_[1].ms, 3),
+                       "a_values_read": "FP32 copy (every value of A exact in FP32; FP64 products, bit-identical "
+                                        "iterates)" if hi_[1].a_fp32 else "FP64",
                        "rel_res": relres_head,
                        "plain_fp64_ms": round(plain_v, 3), "plain_fp64_iters": pl_[1].iters,
                        "plain_fp64_build_ms": round(pl_[0].ms, 3), "plain_rel_res": relres_plain,

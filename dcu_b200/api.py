@@ -168,6 +168,11 @@ class Context:
         """Wide-slice pre-pass of later solves on (default) or off (dcu_set_wide_prepass)."""
         self._check(self._L.dcu_set_wide_prepass(self.h, 1 if enabled else 0))
 
+    def set_exact_a32(self, enabled: bool):
+        """A read from its FP32 copy when every value is exact in FP32 (default), or always FP64
+        (dcu_set_exact_a32); the iterates are bit-identical either way."""
+        self._check(self._L.dcu_set_exact_a32(self.h, 1 if enabled else 0))
+
     def autotune_d(self, n, nnz, ptr_d, idx_d, val_d, b_d, reps: int = 10, **opt) -> "N.Tuning":
         """Time the launch configurations of opt's precision form on this matrix and keep the fastest
         for later builds and solves of that form on this context (dcu_autotune_d)."""

@@ -693,6 +693,7 @@ int run_batch(Ctx* c, int nsys, const int* sys_off_d, const SellPlan& plan, cons
     info->status = worst;
     info->replacements = 0;
     info->res = info->true_res = info->bnorm = 0.0;
+    info->a_fp32 = 0;  // the batched kernels read A's FP64 values
     float ms = 0.f;
     cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
     info->ms = ms;

@@ -44,6 +44,7 @@ struct Scal {
   double rho, alpha, omega, beta, res, thr, bnorm, true_res;
   int it, done, status, pidx;
   int verify, verify_pending, maxiter, replacements;
+  int a32;  // the A products read the FP32 copy of A's values (every value exact in FP32)
   unsigned counter[8];
 };
 
@@ -277,6 +278,8 @@ struct BiArgs {
   const int* su;        // per slice flags (SellPlan::su)
   const IT* ix;         // shared by A and M (same pattern)
   const double* aval;
+  const float* aval32;   // FP32 copy of aval, or null
+  const int* a_inexact;  // nonzero when some A value is not exact in FP32
   const MT* mval;
   const MT* mval8;      // narrow slices' M values, row-major (FP32 / BF16 M), or null
   const double* b;
@@ -302,6 +305,17 @@ struct BiArgs {
 template <typename MT, typename IT, typename VT, typename F>
 __device__ __forceinline__ double a_row(const BiArgs<MT, IT, VT>& a, int r, F xf) {
   return sell_row<false, double, IT>(a.off, a.kd, a.kd8, a.kd8h, a.su, a.wide_val, a.aval, nullptr, a.ix, r, xf);
+}
+// The plain FP64 form (FP64 M) never reads A's FP32 copy.
+template <typename MT>
+constexpr bool kA32 = !std::is_same<MT, double>::value;
+
+// A's row from the FP32 copy of its values: the same numbers when every
+// value of A is exact in FP32 (Scal::a32), widened to FP64 before the
+// multiply, so the row's sum is bit-identical to a_row's.
+template <typename MT, typename IT, typename VT, typename F>
+__device__ __forceinline__ double a_row32(const BiArgs<MT, IT, VT>& a, int r, F xf) {
+  return sell_row<false, float, IT>(a.off, a.kd, a.kd8, a.kd8h, a.su, a.wide_val, a.aval32, nullptr, a.ix, r, xf);
 }
 // M's row: narrow slices from the row-major narrow array where the form has one.
 template <typename MT, typename IT, typename VT, typename F>
@@ -474,6 +488,7 @@ __global__ void __launch_bounds__(BI_BLOCK) k_bi_init(BiArgs<MT, IT, VT> a, doub
     S->verify_pending = 0;
     S->replacements = 0;
     S->true_res = -1.0;
+    S->a32 = (a.aval32 && *a.a_inexact == 0) ? 1 : 0;
     S->status = ST_RUN;
     S->done = 0;
     if (S->res == 0.0) {  // x0 already solves the system
@@ -570,11 +585,16 @@ __global__ void __launch_bounds__(BI_BLOCK, (std::is_same<MT, double>::value || 
   if (finished(a.S)) return;
   double v[1] = {0.0};
   const VT* __restrict__ y = a.y;
+  auto yf = [&](int c) { return ldv(y + c); };
   const int stride = gridDim.x * BI_BLOCK;
-  for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) {
-    const double ayv = a_row(a, r, [&](int c) { return ldv(y + c); });
+  auto row = [&](int r, double ayv) {
     a.ay[r] = ayv;
     v[0] += (double)a.rs[r] * ayv;
+  };
+  if (kA32<MT> && a.S->a32) {
+    for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) row(r, a_row32(a, r, yf));
+  } else {
+    for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) row(r, a_row(a, r, yf));
   }
   double tot[1];
   if (grid_reduce<1>(v, a.part, &a.S->counter[1], tot) && threadIdx.x == 0) {
@@ -610,12 +630,17 @@ __global__ void __launch_bounds__(BI_BLOCK) k_bi_az(BiArgs<MT, IT, VT> a) {
   if (finished(a.S)) return;
   double v[2] = {0.0, 0.0};
   const VT* __restrict__ z = a.z;
+  auto zf = [&](int c) { return ldv(z + c); };
   const int stride = gridDim.x * BI_BLOCK;
-  for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) {
-    const double azv = a_row(a, r, [&](int c) { return ldv(z + c); });
+  auto row = [&](int r, double azv) {
     a.az[r] = azv;
     v[0] += azv * a.s[r];
     v[1] += azv * azv;
+  };
+  if (kA32<MT> && a.S->a32) {
+    for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) row(r, a_row32(a, r, zf));
+  } else {
+    for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) row(r, a_row(a, r, zf));
   }
   double tot[2];
   if (grid_reduce<2>(v, a.part, &a.S->counter[2], tot) && threadIdx.x == 0) {
@@ -762,7 +787,7 @@ int grid_for(const Ctx* c, long long items, int per_sm, int sel) {
 }
 
 template <typename MT, typename IT, typename VT>
-int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval, const IT* ix, const double* b,
+int run_solver(Ctx* c, const SellPlan& plan, const SellA& aval, const MT* mval, const IT* ix, const double* b,
                double* x, const dcu_options* opt, const dcu_tuning* tu, dcu_solve_info* info,
                const MT* mval8 = nullptr) {
   const int n = plan.n;
@@ -829,7 +854,9 @@ int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval,
   a.kd8h = plan.kd8h;
   a.su = plan.su;
   a.ix = ix;
-  a.aval = aval;
+  a.aval = aval.v64;
+  a.aval32 = aval.v32;
+  a.a_inexact = aval.inexact;
   a.mval = mval;
   a.mval8 = mval8;
   a.b = b;
@@ -1009,6 +1036,7 @@ int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval,
     info->res = hs.res;
     info->true_res = hs.true_res;
     info->bnorm = hs.bnorm;
+    info->a_fp32 = hs.a32;
     float ms = 0.f;
     cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
     info->ms = ms;
@@ -1018,7 +1046,7 @@ int run_solver(Ctx* c, const SellPlan& plan, const double* aval, const MT* mval,
 
 }  // namespace
 
-int bicgstab_solve(Ctx* c, const SellPlan& plan, const double* aval_sell, const void* mval_sell, const double* b,
+int bicgstab_solve(Ctx* c, const SellPlan& plan, const SellA& aval_sell, const void* mval_sell, const double* b,
                    double* x, const dcu_options* opt, dcu_solve_info* info, const void* mval8_sell) {
   const int p = opt->precision;
   const dcu_tuning* tu = (p >= 0 && p < 5 && c->tune_set[p]) ? &c->tune[p] : nullptr;

@@ -55,11 +55,22 @@ int resolve_range(Ctx* c, int n, const dcu_options* in, dcu_options* out) {
   return DCU_OK;
 }
 
-// A's values (FP64) in SELL order.
-int gather_a(Ctx* c, const dcu::SellPlan& plan, const double* val) {
+// A's values (FP64) in SELL order, and for the forms other than plain FP64
+// (which reads FP64 values, as it reads int32 indices), unless
+// dcu_set_exact_a32 turned it off, the FP32 copy with its exactness flag.
+int gather_a(Ctx* c, const dcu::SellPlan& plan, const double* val, int precision, dcu::SellA* a) {
   const size_t slots = (size_t)(plan.slots > 0 ? plan.slots : 1);
   DCU_TRY(dcu::ensure(c, dcu::B_SELL_AVAL, sizeof(double) * slots));
-  return dcu::sell_gather_f64(c, plan, val, dcu::bp<double>(c, dcu::B_SELL_AVAL));
+  *a = dcu::SellA{};
+  a->v64 = dcu::bp<double>(c, dcu::B_SELL_AVAL);
+  if (!c->exact_a32 || precision == DCU_PREC_FP64)
+    return dcu::sell_gather_f64(c, plan, val, dcu::bp<double>(c, dcu::B_SELL_AVAL));
+  DCU_TRY(dcu::ensure(c, dcu::B_SELL_AVAL32, sizeof(float) * slots));
+  DCU_TRY(dcu::ensure(c, dcu::B_SELL_AFLAG, sizeof(int)));
+  a->v32 = dcu::bp<float>(c, dcu::B_SELL_AVAL32);
+  a->inexact = dcu::bp<int>(c, dcu::B_SELL_AFLAG);
+  return dcu::sell_gather_a(c, plan, val, dcu::bp<double>(c, dcu::B_SELL_AVAL), dcu::bp<float>(c, dcu::B_SELL_AVAL32),
+                            dcu::bp<int>(c, dcu::B_SELL_AFLAG));
 }
 
 // M's values (by form) in SELL order; an FP32 / BF16 M's narrow slices
@@ -88,10 +99,10 @@ int gather_m(Ctx* c, const dcu::SellPlan& pl, const double* mval, int precision,
   return DCU_OK;
 }
 
-// A's values (FP64) and M's (by form) in SELL order.
+// A's values and M's (by form) in SELL order.
 int gather_values(Ctx* c, const dcu::SellPlan& plan, const double* val, const double* mval, int precision,
-                  const void** msell, const void** msell8) {
-  DCU_TRY(gather_a(c, plan, val));
+                  dcu::SellA* asell, const void** msell, const void** msell8) {
+  DCU_TRY(gather_a(c, plan, val, precision, asell));
   return gather_m(c, plan, mval, precision, msell, msell8);
 }
 
@@ -106,9 +117,9 @@ struct OnStream {
 
 // Solver-side layout of A and M: SELL plan + values.
 int prepare_solve(Ctx* c, int n, int nnz, const int* ptr, const int* idx, const double* val, const double* mval,
-                  int precision, dcu::SellPlan* plan, const void** msell, const void** msell8) {
+                  int precision, dcu::SellPlan* plan, dcu::SellA* asell, const void** msell, const void** msell8) {
   DCU_TRY(dcu::sell_plan(c, n, nnz, ptr, idx, plan));
-  return gather_values(c, *plan, val, mval, precision, msell, msell8);
+  return gather_values(c, *plan, val, mval, precision, asell, msell, msell8);
 }
 
 // The whole path on device arrays: validation, the SELL plan (pattern only),
@@ -139,12 +150,13 @@ int solve_pipeline(Ctx* c, int n, int nnz, const int* ptr, const int* idx, const
   // values in SELL order on the auxiliary stream, whose host round trips wait
   // for that stream alone.
   dcu::SellPlan plan;
+  dcu::SellA asell;
   {
     OnStream aux(c, c->aux_stream);
     DCU_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev[6], 0));
     DCU_TRY(dcu::sell_plan(c, n, nnz, ptr, idx, &plan));
     if (val_ready) DCU_CUDA(c, cudaStreamWaitEvent(c->stream, val_ready, 0));
-    DCU_TRY(gather_a(c, plan, val));
+    DCU_TRY(gather_a(c, plan, val, o.precision, &asell));
     DCU_CUDA(c, cudaEventRecord(c->ev[7], c->stream));
   }
   DCU_TRY(dcu::spai_build_finish(c, &job, &bl));
@@ -153,7 +165,7 @@ int solve_pipeline(Ctx* c, int n, int nnz, const int* ptr, const int* idx, const
   const void *msell = nullptr, *msell8 = nullptr;
   DCU_TRY(gather_m(c, plan, m, o.precision, &msell, &msell8));
   if (bx_ready) DCU_CUDA(c, cudaStreamWaitEvent(c->stream, bx_ready, 0));
-  DCU_TRY(dcu::bicgstab_solve(c, plan, dcu::bp<double>(c, dcu::B_SELL_AVAL), msell, b, x, &o, sinfo, msell8));
+  DCU_TRY(dcu::bicgstab_solve(c, plan, asell, msell, b, x, &o, sinfo, msell8));
   DCU_CUDA(c, cudaEventSynchronize(c->ev[5]));
   cudaEventElapsedTime(&bl.ms, c->ev[4], c->ev[5]);
   if (binfo) *binfo = bl;
@@ -636,10 +648,11 @@ int dcu_bicgstab_d(dcu_spai_ctx* c, int n, int nnz, const int* ptr, const int* i
   try {
     StreamScope scope(c);
     dcu::SellPlan plan;
+    dcu::SellA asell;
     const void *msell = nullptr, *msell8 = nullptr;
     DCU_TRY(dcu::validate_csc(c, n, nnz, ptr, idx));
-    DCU_TRY(prepare_solve(c, n, nnz, ptr, idx, val, mval, o.precision, &plan, &msell, &msell8));
-    return dcu::bicgstab_solve(c, plan, dcu::bp<double>(c, dcu::B_SELL_AVAL), msell, b, x, &o, info, msell8);
+    DCU_TRY(prepare_solve(c, n, nnz, ptr, idx, val, mval, o.precision, &plan, &asell, &msell, &msell8));
+    return dcu::bicgstab_solve(c, plan, asell, msell, b, x, &o, info, msell8);
   } catch (const std::bad_alloc&) {
     return dcu::fail(c, DCU_ERR_ALLOC, "host allocation failed");
   }
@@ -692,9 +705,10 @@ int dcu_bicgstab_transpose_d(dcu_spai_ctx* c, int n, int nnz, const int* ptr, co
     // A's CSC arrays are the CSR arrays of A^T (and of M^T: same pattern)
     dcu::SellPlan plan;
     DCU_TRY(dcu::sell_plan_rows(c, n, nnz, ptr, idx, &plan));
+    dcu::SellA asell;
     const void *msell = nullptr, *msell8 = nullptr;
-    DCU_TRY(gather_values(c, plan, val, mval, o.precision, &msell, &msell8));
-    return dcu::bicgstab_solve(c, plan, dcu::bp<double>(c, dcu::B_SELL_AVAL), msell, b, x, &o, info, msell8);
+    DCU_TRY(gather_values(c, plan, val, mval, o.precision, &asell, &msell, &msell8));
+    return dcu::bicgstab_solve(c, plan, asell, msell, b, x, &o, info, msell8);
   } catch (const std::bad_alloc&) {
     return dcu::fail(c, DCU_ERR_ALLOC, "host allocation failed");
   }
@@ -741,9 +755,10 @@ int dcu_batch_solve_d(dcu_spai_ctx* c, int nsys, const int* sys_off, int n, int 
     cudaEventElapsedTime(&bl.ms, c->ev[0], c->ev[1]);
     if (binfo) *binfo = bl;
     dcu::SellPlan plan;
+    dcu::SellA asell;
     const void *msell = nullptr, *msell8 = nullptr;
-    DCU_TRY(prepare_solve(c, n, nnz, ptr, idx, val, m, DCU_PREC_FP64, &plan, &msell, &msell8));
-    return dcu::batch_solve(c, nsys, sys_off, plan, dcu::bp<double>(c, dcu::B_SELL_AVAL), (const double*)msell,
+    DCU_TRY(prepare_solve(c, n, nnz, ptr, idx, val, m, DCU_PREC_FP64, &plan, &asell, &msell, &msell8));
+    return dcu::batch_solve(c, nsys, sys_off, plan, asell.v64, (const double*)msell,
                             nrhs, B, X, &o, iters, status, sinfo);
   } catch (const std::bad_alloc&) {
     return dcu::fail(c, DCU_ERR_ALLOC, "host allocation failed");
@@ -759,6 +774,12 @@ int dcu_sell_plan_stats(dcu_spai_ctx* c, long long* slots, long long* uniform_sl
 int dcu_set_wide_prepass(dcu_spai_ctx* c, int enabled) {
   if (!c) return DCU_ERR_ARG;
   c->wide_prepass = enabled != 0;
+  return DCU_OK;
+}
+
+int dcu_set_exact_a32(dcu_spai_ctx* c, int enabled) {
+  if (!c) return DCU_ERR_ARG;
+  c->exact_a32 = enabled != 0;
   return DCU_OK;
 }
 

@@ -59,6 +59,8 @@ enum BufId {
   B_WIDEVAL,       // solver: row values of those slices, from the wide pre-pass
   B_SELL_KD8,      // SELL: per narrow slice, its (up to 8) column offsets (int32, then int16)
   B_SELL_MVAL8,    // M values (FP32 / BF16) of the narrow slices, 8 per row, row-major
+  B_SELL_AVAL32,   // A values in SELL order, FP32 copy (used when every value is exact in FP32)
+  B_SELL_AFLAG,    // int: nonzero when some A value is not exactly an FP32 number
   B_COUNT
 };
 
@@ -117,6 +119,7 @@ struct Ctx {
   int profile_default_split = 0;   // the form's default first step
   int plan_wide = 0;               // slices of the last SELL plan wider than kWideSlice
   bool wide_prepass = true;        // flag wide slices for the pre-pass (dcu_set_wide_prepass)
+  bool exact_a32 = true;           // A read from its FP32 copy when exact (dcu_set_exact_a32)
 };
 
 // Iteration kernels of BiCGSTAB, for profiling and the autotuner.
@@ -224,6 +227,9 @@ int sampled_outer(Ctx* c, int n, const int* ptr, const int* idx, const double* u
                   double* out);
 // dst[slot] = (perm[slot] >= 0) ? src[perm[slot]] : 0, converted to the element type.
 int sell_gather_f64(Ctx* c, const SellPlan& p, const double* src, double* dst);
+// A's values in SELL order (dst) and an FP32 copy (dst32); *inexact (zeroed
+// here) becomes nonzero when some value is not exactly an FP32 number.
+int sell_gather_a(Ctx* c, const SellPlan& p, const double* src, double* dst, float* dst32, int* inexact);
 int sell_gather_f32(Ctx* c, const SellPlan& p, const double* src, float* dst);
 int sell_gather_bf16(Ctx* c, const SellPlan& p, const double* src, __nv_bfloat16* dst);
 // An FP32 / BF16 M for the solver: the values of the narrow slices row-major,
@@ -273,9 +279,17 @@ int spai_pattern(Ctx* c, int n, const int* ptr, const int* idx, int col_start, i
 // ---------------------------------------------------------------------------
 // BiCGSTAB on the SELL plan.
 // ---------------------------------------------------------------------------
+// A's values in SELL order: FP64 (v64), and an FP32 copy (v32, or NULL) that
+// the A products read instead when the device flag *inexact is zero.  The
+// FP32 copy then holds the same numbers, so the iterates are bit-identical.
+struct SellA {
+  const double* v64 = nullptr;
+  const float* v32 = nullptr;
+  const int* inexact = nullptr;
+};
 // mval8_sell: an FP32 / BF16 M's narrow-slice values (sell_gather_m8_*), or
 // NULL (every slice then read from mval_sell).
-int bicgstab_solve(Ctx* c, const SellPlan& plan, const double* aval_sell, const void* mval_sell,
+int bicgstab_solve(Ctx* c, const SellPlan& plan, const SellA& aval_sell, const void* mval_sell,
                    const double* b, double* x, const dcu_options* opt, dcu_solve_info* info,
                    const void* mval8_sell = nullptr);
 void release_graphs(Ctx* c);

@@ -355,6 +355,25 @@ __global__ void k_sell_gather(const int* __restrict__ sperm, long long slots, co
   }
 }
 
+// A's values: the FP64 SELL copy, an FP32 copy, and a flag raised (one
+// atomic per warp) when a value does not survive the round trip through FP32
+// bit for bit (a rounded value, an FP64 subnormal, a value beyond FP32's
+// range, a NaN payload).
+__global__ void k_sell_gather_a(const int* __restrict__ sperm, long long slots, const double* __restrict__ src,
+                                double* __restrict__ dst, float* __restrict__ dst32, int* __restrict__ inexact) {
+  bool off = false;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < slots;
+       q += (long long)gridDim.x * blockDim.x) {
+    const int p = sperm[q];
+    const double v = p >= 0 ? src[p] : 0.0;
+    const float f = __double2float_rn(v);
+    dst[q] = v;
+    dst32[q] = f;
+    off |= __double_as_longlong((double)f) != __double_as_longlong(v);
+  }
+  if (__any_sync(0xffffffffu, off) && (threadIdx.x & 31) == 0) atomicOr(inexact, 1);
+}
+
 template <typename T>
 int sell_gather(Ctx* c, const SellPlan& p, const double* src, T* dst) {
   int grid = waves_grid(c, p.slots, 256, 8);
@@ -638,6 +657,13 @@ int plan_stats(Ctx* c, long long* slots, long long* uniform_slots, long long* wi
 }
 
 int sell_gather_f64(Ctx* c, const SellPlan& p, const double* src, double* dst) { return sell_gather<double>(c, p, src, dst); }
+int sell_gather_a(Ctx* c, const SellPlan& p, const double* src, double* dst, float* dst32, int* inexact) {
+  DCU_CUDA(c, cudaMemsetAsync(inexact, 0, sizeof(int), c->stream));
+  int grid = waves_grid(c, p.slots, 256, 8);
+  k_sell_gather_a<<<grid, 256, 0, c->stream>>>(p.perm, p.slots, src, dst, dst32, inexact);
+  DCU_LAUNCHED(c, "k_sell_gather_a");
+  return DCU_OK;
+}
 int sell_gather_f32(Ctx* c, const SellPlan& p, const double* src, float* dst) { return sell_gather<float>(c, p, src, dst); }
 int sell_gather_bf16(Ctx* c, const SellPlan& p, const double* src, __nv_bfloat16* dst) {
   return sell_gather<__nv_bfloat16>(c, p, src, dst);

@@ -41,7 +41,7 @@ class BuildInfo(C.Structure):
 
 class SolveInfo(C.Structure):
     _fields_ = [("iters", C.c_int), ("status", C.c_int), ("replacements", C.c_int), ("res", C.c_double),
-                ("true_res", C.c_double), ("bnorm", C.c_double), ("ms", C.c_float)]
+                ("true_res", C.c_double), ("bnorm", C.c_double), ("ms", C.c_float), ("a_fp32", C.c_int)]
 
 
 class Tuning(C.Structure):
@@ -91,6 +91,7 @@ SIGNATURES = {
     "dcu_profile_iteration_kernels": (_i, [_vp, _i, C.POINTER(C.c_float), _i, C.POINTER(_i)]),
     "dcu_sell_plan_stats": (_i, [_vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     "dcu_set_wide_prepass": (_i, [_vp, _i]),
+    "dcu_set_exact_a32": (_i, [_vp, _i]),
     "dcu_tuning_default": (None, [C.POINTER(Tuning)]),
     "dcu_set_tuning": (_i, [_vp, _i, C.POINTER(Tuning)]),
     "dcu_get_tuning": (_i, [_vp, _i, C.POINTER(Tuning)]),

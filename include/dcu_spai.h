@@ -125,6 +125,9 @@ typedef struct {
   double true_res;        /* ||b - A x||_2 recomputed in FP64 at exit                  */
   double bnorm;           /* ||b||_2                                                   */
   float ms;               /* device time of the solve (CUDA events)                   */
+  int a_fp32;             /* 1 when the A products read A's FP32 copy (a form other than
+                             DCU_PREC_FP64, every value of A exact in FP32;
+                             dcu_set_exact_a32)                                        */
 } dcu_solve_info;
 
 typedef struct {
@@ -308,6 +311,18 @@ int dcu_sell_plan_stats(dcu_spai_ctx* ctx, long long* slots, long long* uniform_
  * two give bit-identical iterates; off exists to show that, and to time the
  * pre-pass.  No counterpart in the reference. */
 int dcu_set_wide_prepass(dcu_spai_ctx* ctx, int enabled);
+
+/* Let this context's later solves in the forms other than DCU_PREC_FP64 read
+ * A's values from an FP32 copy when every value of A is exactly an FP32
+ * number (enabled != 0, the default), or always from the FP64 array (0).
+ * The check runs on the device while A is laid out for the solver; the
+ * products are formed in FP64 from the same numbers either way, so the
+ * iterates are bit-identical, and a matrix with one value that FP32 rounds
+ * keeps the FP64 reads.  Integer and dyadic stencil coefficients qualify;
+ * values read from decimal text usually do not.  The plain FP64 form always
+ * reads FP64 values (as it always reads int32 indices).  No counterpart in
+ * the reference. */
+int dcu_set_exact_a32(dcu_spai_ctx* ctx, int enabled);
 
 /* ---- autotuner (no counterpart in the reference) ----------------------------- */
 

@@ -209,3 +209,61 @@ def test_wide_prepass_keeps_iterates_bit_identical(ctx, prec):
     assert out[0][1] == out[1][1]
     assert np.array_equal(out[0][0], out[1][0])
     assert out[0][2] == out[1][2]
+
+
+def _dyadic_circuit():
+    """circuit_like with every value rounded up in magnitude to a multiple of
+    1/8: exact in FP32, and its hub rows still make wide slices."""
+    A = W.circuit_like()
+    v = np.sign(A.val) * np.ceil(np.abs(A.val) * 8.0) / 8.0
+    return W.CSC(A.n, A.ptr, A.idx, v)
+
+
+def _one_value_off():
+    """An integer stencil with one value moved by 2^-30: FP32 rounds that one
+    value, so the whole matrix must keep the FP64 reads."""
+    A = W.convdiff3d(24, 20.0)
+    v = A.val.copy()
+    v[len(v) // 2] += 2.0 ** -30
+    return W.CSC(A.n, A.ptr, A.idx, v)
+
+
+EXACT_A32_CASES = {
+    "stencil3d_integer": (lambda: W.convdiff3d(24, 20.0), 1),
+    "circuit_dyadic_wide": (_dyadic_circuit, 1),
+    "stencil3d_one_value_off": (_one_value_off, 0),
+    "varcoef_inexact": (lambda: W.varcoef2d(64, seed=3), 0),
+}
+
+
+@pytest.mark.parametrize("case", list(EXACT_A32_CASES))
+@pytest.mark.parametrize("prec", [N.PREC_FP64, N.PREC_M_BF16])
+def test_exact_fp32_a_keeps_iterates_bit_identical(ctx, case, prec):
+    """A's FP32 copy is read only when every value of A is exact in FP32, and
+    then it holds the same numbers: the iterates, the count and the residuals
+    equal those of the FP64 reads bit for bit.  A single value that FP32
+    rounds keeps the whole solve on the FP64 reads (a_fp32 = 0); if it did
+    not, that value would change and the bits with it.  The plain FP64 form
+    never reads the copy."""
+    import torch
+
+    make, expect = EXACT_A32_CASES[case]
+    if prec == N.PREC_FP64:
+        expect = 0
+    A = make()
+    rng = np.random.Generator(np.random.PCG64(17))
+    b = rng.uniform(-1, 1, A.n)
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    ptr, idx, val, bd = d(A.ptr), d(A.idx), d(A.val), d(b)
+    out = []
+    try:
+        for on in (True, False):
+            ctx.set_exact_a32(on)
+            x = torch.zeros(A.n, dtype=torch.float64, device="cuda")
+            _, si = ctx.solve_d(A.n, A.nnz, ptr, idx, val, bd, x, precision=prec, maxiter=2000)
+            assert si.a_fp32 == (expect if on else 0)
+            out.append((x.cpu().numpy(), si.iters, si.status, si.res, si.true_res))
+    finally:
+        ctx.set_exact_a32(True)
+    assert out[0][1:] == out[1][1:]
+    assert np.array_equal(out[0][0], out[1][0])
