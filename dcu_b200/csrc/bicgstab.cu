@@ -587,14 +587,23 @@ __global__ void __launch_bounds__(BI_BLOCK, (std::is_same<MT, double>::value || 
   const VT* __restrict__ y = a.y;
   auto yf = [&](int c) { return ldv(y + c); };
   const int stride = gridDim.x * BI_BLOCK;
-  auto row = [&](int r, double ayv) {
+  // r*[r] is loaded with the row's values, not after the store of Ay[r]
+  // (which the load could alias): one round trip per row instead of two
+  auto row = [&](int r, double rsv, double ayv) {
     a.ay[r] = ayv;
-    v[0] += (double)a.rs[r] * ayv;
+    v[0] += rsv * ayv;
   };
+  const VT* __restrict__ rs = a.rs;
   if (kA32<MT> && a.S->a32) {
-    for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) row(r, a_row32(a, r, yf));
+    for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) {
+      const double rsv = ldv(rs + r);
+      row(r, rsv, a_row32(a, r, yf));
+    }
   } else {
-    for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) row(r, a_row(a, r, yf));
+    for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) {
+      const double rsv = ldv(rs + r);
+      row(r, rsv, a_row(a, r, yf));
+    }
   }
   double tot[1];
   if (grid_reduce<1>(v, a.part, &a.S->counter[1], tot) && threadIdx.x == 0) {
@@ -618,8 +627,10 @@ __global__ void __launch_bounds__(BI_BLOCK) k_bi_sz(BiArgs<MT, IT, VT> a) {
   auto sf = [&](int c) { return ldv(rr + c) + nalpha * ldv(ay + c); };
   const int stride = gridDim.x * BI_BLOCK;
   for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) {
+    // the row's own r and Ay load with its values, not after the SpMV
+    const double rv = ldv(rr + r), ayv = ldv(ay + r);
     const double zv = m_row(a, r, sf);
-    a.s[r] = rr[r] + nalpha * ay[r];
+    a.s[r] = rv + nalpha * ayv;
     a.z[r] = (VT)zv;
   }
 }
@@ -632,15 +643,24 @@ __global__ void __launch_bounds__(BI_BLOCK) k_bi_az(BiArgs<MT, IT, VT> a) {
   const VT* __restrict__ z = a.z;
   auto zf = [&](int c) { return ldv(z + c); };
   const int stride = gridDim.x * BI_BLOCK;
-  auto row = [&](int r, double azv) {
+  // s[r] is loaded with the row's values, not after the store of Az[r]
+  // (which the load could alias): one round trip per row instead of two
+  auto row = [&](int r, double sv, double azv) {
     a.az[r] = azv;
-    v[0] += azv * a.s[r];
+    v[0] += azv * sv;
     v[1] += azv * azv;
   };
+  const double* __restrict__ s = a.s;
   if (kA32<MT> && a.S->a32) {
-    for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) row(r, a_row32(a, r, zf));
+    for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) {
+      const double sv = ldv(s + r);
+      row(r, sv, a_row32(a, r, zf));
+    }
   } else {
-    for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) row(r, a_row(a, r, zf));
+    for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) {
+      const double sv = ldv(s + r);
+      row(r, sv, a_row(a, r, zf));
+    }
   }
   double tot[2];
   if (grid_reduce<2>(v, a.part, &a.S->counter[2], tot) && threadIdx.x == 0) {
