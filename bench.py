@@ -88,11 +88,11 @@ def bytes_per_kernel(n, nnz, w_m, w_v, ib, split, w_a=8):
 # DRAM bytes (read + write: dram__bytes_read.sum + dram__bytes_write.sum) of
 # one launch of each iteration kernel at 128^3, recorded from one ncu capture
 # per kernel (cold L2, single launch; the summary under profiles/ gives the
-# command), keyed by (kernel, form).  A constant: ncu does not run inside the
-# benchmark.
+# command), keyed by (kernel, form); K2 and K4 of m_bf16 read A's exact FP32
+# copy.  A constant: ncu does not run inside the benchmark.
 TRAFFIC_BYTES = {
-    ("k_bi_p", "m_bf16"): 50.38e6, ("k_bi_y", "m_bf16"): 52.99e6, ("k_bi_ay", "m_bf16"): 157.94e6,
-    ("k_bi_sz", "m_bf16"): 73.30e6, ("k_bi_az", "m_bf16"): 156.71e6, ("k_bi_xr", "m_bf16"): 110.28e6,
+    ("k_bi_p", "m_bf16"): 50.38e6, ("k_bi_y", "m_bf16"): 52.99e6, ("k_bi_ay", "m_bf16"): 98.09e6,
+    ("k_bi_sz", "m_bf16"): 73.30e6, ("k_bi_az", "m_bf16"): 97.40e6, ("k_bi_xr", "m_bf16"): 110.28e6,
     ("k_bi_py", "fp64"): 178.59e6,
 }
 
@@ -575,6 +575,13 @@ def main():
                 "sell_slots": slots, "uniform_slots": uslots}
     it_us = inf_head[-1][1].ms * 1e3 / max(1, inf_head[-1][1].iters)
     it_gbs = sum(kbytes) / (it_us * 1e-6) / 1e9
+    # the dominant kernel's share of the single-launch times applied to the
+    # iteration measured inside the solve (graph, programmatic dependent
+    # launch): its time without the launch latency that a single launch
+    # between two events also holds
+    in_us = kms[j] / sum(kms) * it_us
+    roofline["in_solve_estimate"] = {"us": round(in_us, 2), "achieved": round(kbytes[j] / (in_us * 1e-6) / 1e9, 1),
+                                     "frac": round(kbytes[j] / (in_us * 1e-6) / 1e9 / peak, 3)}
     roofline["iteration"] = {"bytes": int(sum(kbytes)), "us": round(it_us, 1), "achieved": round(it_gbs, 1),
                              "frac": round(it_gbs / peak, 3)}
     # the plain FP64 form's iteration on the same layout, and both forms' whole
