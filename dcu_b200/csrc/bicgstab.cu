@@ -456,9 +456,12 @@ template <typename MT, typename IT, typename VT>
 __global__ void __launch_bounds__(BI_BLOCK) k_bi_init(BiArgs<MT, IT, VT> a, double tol, int tol_mode, int maxiter,
                                                       int verify) {
   double v[3] = {0.0, 0.0, 0.0};
+  // with every value of A exact in FP32 its FP64 SELL copy may be absent
+  const bool a32 = kA32<MT> && a.aval32 && *a.a_inexact == 0;
+  auto xf = [&](int c) { return ldv(a.x + c); };
   const int stride = gridDim.x * BI_BLOCK;
   for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) {
-    const double ax = a_row(a, r, [&](int c) { return ldv(a.x + c); });
+    const double ax = a32 ? a_row32(a, r, xf) : a_row(a, r, xf);
     const double br = a.b[r];
     const double rr = br + (-1.0) * ax;
     a.r[r] = rr;
@@ -750,9 +753,11 @@ __global__ void __launch_bounds__(BI_BLOCK, 6) k_bi_xr(BiArgs<MT, IT, VT> a) {
 template <typename MT, typename IT, typename VT>
 __global__ void __launch_bounds__(BI_BLOCK) k_bi_true(BiArgs<MT, IT, VT> a, int replace) {
   double v[2] = {0.0, 0.0};
+  const bool a32 = kA32<MT> && a.S->a32;  // (k_bi_init decided it)
+  auto xf = [&](int c) { return ldv(a.x + c); };
   const int stride = gridDim.x * BI_BLOCK;
   for (int r = blockIdx.x * BI_BLOCK + threadIdx.x; r < a.n; r += stride) {
-    const double ax = a_row(a, r, [&](int c) { return ldv(a.x + c); });
+    const double ax = a32 ? a_row32(a, r, xf) : a_row(a, r, xf);
     const double rt = a.b[r] - ax;
     if (replace) a.r[r] = rt;
     v[0] += (double)a.rs[r] * rt;

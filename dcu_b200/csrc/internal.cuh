@@ -227,8 +227,9 @@ int sampled_outer(Ctx* c, int n, const int* ptr, const int* idx, const double* u
                   double* out);
 // dst[slot] = (perm[slot] >= 0) ? src[perm[slot]] : 0, converted to the element type.
 int sell_gather_f64(Ctx* c, const SellPlan& p, const double* src, double* dst);
-// A's values in SELL order (dst) and an FP32 copy (dst32); *inexact (zeroed
-// here) becomes nonzero when some value is not exactly an FP32 number.
+// A's values in SELL order as an FP32 copy (dst32); *inexact (zeroed here)
+// becomes nonzero when some value is not exactly an FP32 number, and only
+// then, or when the plan has wide slices, is the FP64 copy (dst) written.
 int sell_gather_a(Ctx* c, const SellPlan& p, const double* src, double* dst, float* dst32, int* inexact);
 int sell_gather_f32(Ctx* c, const SellPlan& p, const double* src, float* dst);
 int sell_gather_bf16(Ctx* c, const SellPlan& p, const double* src, __nv_bfloat16* dst);
@@ -281,7 +282,9 @@ int spai_pattern(Ctx* c, int n, const int* ptr, const int* idx, int col_start, i
 // ---------------------------------------------------------------------------
 // A's values in SELL order: FP64 (v64), and an FP32 copy (v32, or NULL) that
 // the A products read instead when the device flag *inexact is zero.  The
-// FP32 copy then holds the same numbers, so the iterates are bit-identical.
+// FP32 copy then holds the same numbers, so the iterates are bit-identical;
+// v64 is then written only for a plan with wide slices (whose pre-pass reads
+// it).
 struct SellA {
   const double* v64 = nullptr;
   const float* v32 = nullptr;

@@ -47,11 +47,58 @@ __global__ void k_row_scatter(const int* __restrict__ ptr, const int* __restrict
 __global__ void k_csr_symmetric(const int* __restrict__ ptr, const int* __restrict__ idx, int n,
                                 int* __restrict__ rptr, int* __restrict__ rcol, int* __restrict__ rperm,
                                 int* __restrict__ flag) {
+  constexpr int kShort = 8;  // columns up to this long search their partners side by side
   int bad = 0;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
     const int s = ptr[c], e = ptr[c + 1];
     rptr[c] = s;
     if (c == n - 1) rptr[n] = e;
+    if (e - s <= kShort) {
+      // the entries' rows, their columns' ranges, then the binary searches
+      // one step at a time for all entries: a few dependent loads per column
+      // instead of a few per entry
+      const int len = e - s;
+      int r[kShort], lo[kShort], hi[kShort], q[kShort];
+#pragma unroll
+      for (int t = 0; t < kShort; ++t) r[t] = (t < len) ? idx[s + t] : 0;
+      int prev = -1;
+#pragma unroll
+      for (int t = 0; t < kShort; ++t) {
+        if (t < len) {
+          rcol[s + t] = r[t];
+          if (r[t] <= prev) bad |= 1;
+          prev = r[t];
+          lo[t] = ptr[r[t]];
+          hi[t] = ptr[r[t] + 1] - 1;
+        } else {
+          lo[t] = 0;
+          hi[t] = -1;
+        }
+        q[t] = -1;
+      }
+      for (;;) {
+        bool active = false;
+#pragma unroll
+        for (int t = 0; t < kShort; ++t) {
+          if (q[t] < 0 && lo[t] <= hi[t]) {
+            active = true;
+            const int mid = (lo[t] + hi[t]) >> 1;
+            const int v = idx[mid];
+            if (v == c) q[t] = mid;
+            else if (v < c) lo[t] = mid + 1;
+            else hi[t] = mid - 1;
+          }
+        }
+        if (!active) break;
+      }
+#pragma unroll
+      for (int t = 0; t < kShort; ++t)
+        if (t < len) {
+          if (q[t] < 0) bad |= 2;
+          rperm[s + t] = q[t];
+        }
+      continue;
+    }
     int prev = -1;
     for (int k = s; k < e; ++k) {
       const int r = idx[k];
@@ -296,6 +343,10 @@ __global__ void k_sell_desc(const int* __restrict__ sidx, int n, int nslices, co
                             int* __restrict__ kd, int* __restrict__ su, unsigned long long* __restrict__ uslots,
                             const int* __restrict__ rptr, int* __restrict__ wide, int allow_wide,
                             int* __restrict__ kd8, int16_t* __restrict__ kd8h) {
+  __shared__ unsigned long long blk_uslots;
+  if (threadIdx.x == 0) blk_uslots = 0ull;
+  __syncthreads();
+  unsigned long long my_uslots = 0ull;  // lane 0 of each warp: uniform slots of its slices
   const int rows_total = nslices * 32;
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows_total; r += gridDim.x * blockDim.x) {
     const int s = r >> 5, lane = r & 31;
@@ -303,14 +354,23 @@ __global__ void k_sell_desc(const int* __restrict__ sidx, int n, int nslices, co
     const int w = (int)((off[s + 1] - o0) >> 5);
     bool all = true;
     int my_d = 0;  // lane k < kNarrow: offset of entry position k
-    for (int k = 0; k < w; ++k) {
-      const int d = sidx[o0 + 32ll * k + lane] - r;
+    // position k of the slice (w is the same for the whole warp)
+    auto position = [&](int k, int col) {
+      const int d = col - r;
       const int d0 = __shfl_sync(0xffffffffu, d, 0);  // row 32 s < n always
       const bool same = __all_sync(0xffffffffu, r >= n || d == d0);
       all = all && same;
       if (lane == 0) kd[(o0 >> 5) + k] = same ? (int)(((unsigned)d0 << 1) | 1u) : 0;
       if (lane == k) my_d = d0;
-    }
+    };
+    // the first kNarrow positions' columns are loaded together
+    int pre[kNarrow];
+#pragma unroll
+    for (int k = 0; k < kNarrow; ++k) pre[k] = (k < w) ? sidx[o0 + 32ll * k + lane] : 0;
+#pragma unroll
+    for (int k = 0; k < kNarrow; ++k)
+      if (k < w) position(k, pre[k]);
+    for (int k = kNarrow; k < w; ++k) position(k, sidx[o0 + 32ll * k + lane]);
     const bool narrow = all && w > 0 && w <= kNarrow;
     if (lane < kNarrow) {
       const int d = (narrow && lane < w) ? my_d : 0;
@@ -331,9 +391,14 @@ __global__ void k_sell_desc(const int* __restrict__ sidx, int n, int nslices, co
         f |= 4 | (i << 3);
       }
       su[s] = f;
-      if (all && w > 0) atomicAdd(uslots, 32ull * (unsigned long long)w);
+      if (all && w > 0) my_uslots += 32ull * (unsigned long long)w;
     }
   }
+  // one atomic per block (the warps' loop trip counts differ: no barrier
+  // inside the loop; lane 0 of each warp adds its total here)
+  if ((threadIdx.x & 31) == 0 && my_uslots) atomicAdd(&blk_uslots, my_uslots);
+  __syncthreads();
+  if (threadIdx.x == 0 && blk_uslots) atomicAdd(uslots, blk_uslots);
 }
 
 template <typename T>
@@ -355,23 +420,35 @@ __global__ void k_sell_gather(const int* __restrict__ sperm, long long slots, co
   }
 }
 
-// A's values: the FP64 SELL copy, an FP32 copy, and a flag raised (one
-// atomic per warp) when a value does not survive the round trip through FP32
-// bit for bit (a rounded value, an FP64 subnormal, a value beyond FP32's
-// range, a NaN payload).
+// A's values: an FP32 SELL copy, and a flag raised (one atomic per warp)
+// when a value does not survive the round trip through FP32 bit for bit (a
+// rounded value, an FP64 subnormal, a value beyond FP32's range, a NaN
+// payload).
 __global__ void k_sell_gather_a(const int* __restrict__ sperm, long long slots, const double* __restrict__ src,
-                                double* __restrict__ dst, float* __restrict__ dst32, int* __restrict__ inexact) {
+                                float* __restrict__ dst32, int* __restrict__ inexact) {
   bool off = false;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < slots;
        q += (long long)gridDim.x * blockDim.x) {
     const int p = sperm[q];
     const double v = p >= 0 ? src[p] : 0.0;
     const float f = __double2float_rn(v);
-    dst[q] = v;
     dst32[q] = f;
     off |= __double_as_longlong((double)f) != __double_as_longlong(v);
   }
   if (__any_sync(0xffffffffu, off) && (threadIdx.x & 31) == 0) atomicOr(inexact, 1);
+}
+
+// The FP64 SELL copy of A's values, needed only when some value is not exact
+// in FP32 or when `force` (the wide-slice pre-pass reads FP64 values): with
+// the flag clear and no force every block returns at once.
+__global__ void k_sell_gather_a64(const int* __restrict__ sperm, long long slots, const double* __restrict__ src,
+                                  double* __restrict__ dst, const int* __restrict__ inexact, int force) {
+  if (!force && *inexact == 0) return;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < slots;
+       q += (long long)gridDim.x * blockDim.x) {
+    const int p = sperm[q];
+    dst[q] = p >= 0 ? src[p] : 0.0;
+  }
 }
 
 template <typename T>
@@ -660,8 +737,10 @@ int sell_gather_f64(Ctx* c, const SellPlan& p, const double* src, double* dst) {
 int sell_gather_a(Ctx* c, const SellPlan& p, const double* src, double* dst, float* dst32, int* inexact) {
   DCU_CUDA(c, cudaMemsetAsync(inexact, 0, sizeof(int), c->stream));
   int grid = waves_grid(c, p.slots, 256, 8);
-  k_sell_gather_a<<<grid, 256, 0, c->stream>>>(p.perm, p.slots, src, dst, dst32, inexact);
+  k_sell_gather_a<<<grid, 256, 0, c->stream>>>(p.perm, p.slots, src, dst32, inexact);
   DCU_LAUNCHED(c, "k_sell_gather_a");
+  k_sell_gather_a64<<<grid, 256, 0, c->stream>>>(p.perm, p.slots, src, dst, inexact, p.nwide > 0 ? 1 : 0);
+  DCU_LAUNCHED(c, "k_sell_gather_a64");
   return DCU_OK;
 }
 int sell_gather_f32(Ctx* c, const SellPlan& p, const double* src, float* dst) { return sell_gather<float>(c, p, src, dst); }
