@@ -220,7 +220,11 @@ int csr_from_csc(Ctx* c, int n, int nnz, const int* ptr, const int* idx, int* rp
                  int* rperm);
 int csr_values(Ctx* c, int nnz, const int* rperm, const double* val, double* rval);
 int sell_plan(Ctx* c, int n, int nnz, const int* ptr, const int* idx, SellPlan* plan);
-int sell_fill_from_csr(Ctx* c, int n, int nnz, const int* rptr, const int* rcol, const int* rperm, SellPlan* plan);
+// SELL-32 layout of the operator whose CSR is (rptr, rcol, rperm).  With
+// `check` (a device int), its value is read back with the layout's last
+// round trip into *check_out.
+int sell_fill_from_csr(Ctx* c, int n, int nnz, const int* rptr, const int* rcol, const int* rperm, SellPlan* plan,
+                       const int* check = nullptr, int* check_out = nullptr);
 int sell_plan_rows(Ctx* c, int n, int nnz, const int* rptr, const int* rcol, SellPlan* plan);
 // out[e] = alpha * u[idx[e]] * v[col(e)] on a CSC pattern
 int sampled_outer(Ctx* c, int n, const int* ptr, const int* idx, const double* u, const double* v, double alpha,

@@ -316,7 +316,11 @@ __global__ void k_sell_fill(const int* __restrict__ rptr, const int* __restrict_
 }
 
 __global__ void k_sell_delta(const int* __restrict__ sidx, long long slots, int n, int nslices,
-                             const long long* __restrict__ off, int16_t* __restrict__ del) {
+                             const long long* __restrict__ off, int16_t* __restrict__ del,
+                             const int* __restrict__ maxdelta) {
+  // deltas of 16 bits only when every |col - row| < 32768 (k_sell_fill's
+  // maximum); otherwise every block returns at once
+  if (*maxdelta >= 32768) return;
   // slot q belongs to row 32 s + ((q - off[s]) mod 32); recover s by walking
   // per row instead: one thread per (row, k) over whole slices.
   int rows_total = nslices * 32;
@@ -375,7 +379,7 @@ __global__ void k_sell_desc(const int* __restrict__ sidx, int n, int nslices, co
     if (lane < kNarrow) {
       const int d = (narrow && lane < w) ? my_d : 0;
       kd8[(long long)s * kNarrow + lane] = d;
-      if (kd8h) kd8h[(long long)s * kNarrow + lane] = (int16_t)d;  // |d| < 32768 (delta16)
+      if (kd8h) kd8h[(long long)s * kNarrow + lane] = (int16_t)d;  // read only when every |d| < 32768
     }
     // rows of the slice longer than kWideSlice
     const int len = (r < n) ? rptr[r + 1] - rptr[r] : 0;
@@ -578,21 +582,30 @@ int validate_csc(Ctx* c, int n, int nnz, const int* ptr, const int* idx, bool un
   return DCU_OK;
 }
 
-int csr_from_csc(Ctx* c, int n, int nnz, const int* ptr, const int* idx, int* rptr, int* rcol, int* rperm) {
+namespace {
+
+// k_csr_symmetric into (rptr, rcol, rperm) without waiting: *flag (device) is
+// 0 when the pattern was symmetric with ascending columns and the result
+// stands, else the general path must run.
+int csr_try_symmetric(Ctx* c, int n, const int* ptr, const int* idx, int* rptr, int* rcol, int* rperm,
+                      int** flag) {
+  DCU_TRY(ensure(c, B_LONGROWS, sizeof(int) * (size_t)(n + 2)));
+  int* longcount = bp<int>(c, B_LONGROWS) + n;
+  DCU_CUDA(c, cudaMemsetAsync(longcount, 0, 2 * sizeof(int), c->stream));
+  k_csr_symmetric<<<waves_grid(c, n, 256, 8), 256, 0, c->stream>>>(ptr, idx, n, rptr, rcol, rperm, longcount);
+  DCU_LAUNCHED(c, "k_csr_symmetric");
+  *flag = longcount;
+  return DCU_OK;
+}
+
+// The general CSC -> CSR: counts, scan, scatter, per-row sort.
+int csr_general(Ctx* c, int n, int nnz, const int* ptr, const int* idx, int* rptr, int* rcol, int* rperm) {
   DCU_TRY(ensure(c, B_ROWCNT, sizeof(int) * (size_t)(n + 1)));
   DCU_TRY(ensure(c, B_LONGROWS, sizeof(int) * (size_t)(n + 2)));
   int* cnt = bp<int>(c, B_ROWCNT);
   int* longrows = bp<int>(c, B_LONGROWS);
   int* longcount = longrows + n;  // [0] = count, [1] = longest length
   DCU_CUDA(c, cudaMemsetAsync(longcount, 0, 2 * sizeof(int), c->stream));
-  if (n > 0 && nnz > 0) {
-    k_csr_symmetric<<<waves_grid(c, n, 256, 8), 256, 0, c->stream>>>(ptr, idx, n, rptr, rcol, rperm, longcount);
-    DCU_LAUNCHED(c, "k_csr_symmetric");
-    DCU_CUDA(c, cudaMemcpyAsync(c->pinned, longcount, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-    DCU_CUDA(c, cudaStreamSynchronize(c->stream));
-    if (*(int*)c->pinned == 0) return DCU_OK;
-    DCU_CUDA(c, cudaMemsetAsync(longcount, 0, 2 * sizeof(int), c->stream));
-  }
   DCU_CUDA(c, cudaMemsetAsync(cnt, 0, sizeof(int) * (size_t)(n + 1), c->stream));
   if (nnz > 0) {
     k_row_count<<<waves_grid(c, nnz, 256, 8), 256, 0, c->stream>>>(idx, nnz, cnt);
@@ -624,6 +637,19 @@ int csr_from_csc(Ctx* c, int n, int nnz, const int* ptr, const int* idx, int* rp
   return DCU_OK;
 }
 
+}  // namespace
+
+int csr_from_csc(Ctx* c, int n, int nnz, const int* ptr, const int* idx, int* rptr, int* rcol, int* rperm) {
+  if (n > 0 && nnz > 0) {
+    int* flag = nullptr;
+    DCU_TRY(csr_try_symmetric(c, n, ptr, idx, rptr, rcol, rperm, &flag));
+    DCU_CUDA(c, cudaMemcpyAsync(c->pinned, flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    DCU_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (*(int*)c->pinned == 0) return DCU_OK;
+  }
+  return csr_general(c, n, nnz, ptr, idx, rptr, rcol, rperm);
+}
+
 int sell_plan(Ctx* c, int n, int nnz, const int* ptr, const int* idx, SellPlan* plan) {
   DCU_TRY(ensure(c, B_RPTR, sizeof(int) * (size_t)(n + 1)));
   DCU_TRY(ensure(c, B_RCOL, sizeof(int) * (size_t)(nnz > 0 ? nnz : 1)));
@@ -631,11 +657,24 @@ int sell_plan(Ctx* c, int n, int nnz, const int* ptr, const int* idx, SellPlan* 
   int* rptr = bp<int>(c, B_RPTR);
   int* rcol = bp<int>(c, B_RCOL);
   int* rperm = bp<int>(c, B_RPERM);
-  DCU_TRY(csr_from_csc(c, n, nnz, ptr, idx, rptr, rcol, rperm));
+  if (n > 0 && nnz > 0) {
+    // the layout is built from the symmetric conversion without waiting for
+    // its verdict, which comes back with the layout's last round trip; a
+    // pattern that is not symmetric (the speculative layout stays in bounds:
+    // its row pointers, columns and slots are A's own) is laid out again
+    // from the general conversion
+    int* flag = nullptr;
+    DCU_TRY(csr_try_symmetric(c, n, ptr, idx, rptr, rcol, rperm, &flag));
+    int bad = 0;
+    DCU_TRY(sell_fill_from_csr(c, n, nnz, rptr, rcol, rperm, plan, flag, &bad));
+    if (bad == 0) return DCU_OK;
+  }
+  DCU_TRY(csr_general(c, n, nnz, ptr, idx, rptr, rcol, rperm));
   return sell_fill_from_csr(c, n, nnz, rptr, rcol, rperm, plan);
 }
 
-int sell_fill_from_csr(Ctx* c, int n, int nnz, const int* rptr, const int* rcol, const int* rperm, SellPlan* plan) {
+int sell_fill_from_csr(Ctx* c, int n, int nnz, const int* rptr, const int* rcol, const int* rperm, SellPlan* plan,
+                       const int* check, int* check_out) {
   int nslices = (n + 31) / 32;
   DCU_TRY(ensure(c, B_SELL_W, sizeof(int) * (size_t)(nslices + 1)));
   DCU_TRY(ensure(c, B_SELL_OFF, sizeof(long long) * (size_t)(nslices + 1)));
@@ -657,19 +696,14 @@ int sell_fill_from_csr(Ctx* c, int n, int nnz, const int* rptr, const int* rcol,
   k_sell_fill<<<waves_grid(c, (long long)nslices * 32, 256, 8), 256, 0, c->stream>>>(rptr, rcol, rperm, n, nslices, off,
                                                                                      sidx, sperm, maxdelta);
   DCU_LAUNCHED(c, "k_sell_fill");
-  DCU_CUDA(c, cudaMemcpyAsync(c->pinned, maxdelta, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-  DCU_CUDA(c, cudaStreamSynchronize(c->stream));
-  int md = *(int*)c->pinned;
-  plan->delta16 = md < 32768;
-  plan->del = nullptr;
-  if (plan->delta16) {
-    DCU_TRY(ensure(c, B_SELL_DEL, sizeof(int16_t) * (size_t)(slots > 0 ? slots : 1)));
-    int16_t* del = bp<int16_t>(c, B_SELL_DEL);
-    k_sell_delta<<<waves_grid(c, (long long)nslices * 32, 256, 8), 256, 0, c->stream>>>(sidx, slots, n, nslices, off,
-                                                                                        del);
-    DCU_LAUNCHED(c, "k_sell_delta");
-    plan->del = del;
-  }
+  // the 16-bit deltas and their offsets table are written unless the
+  // maximum |col - row| rules them out; the host reads that maximum with the
+  // wide-slice count at the end, one round trip for both
+  DCU_TRY(ensure(c, B_SELL_DEL, sizeof(int16_t) * (size_t)(slots > 0 ? slots : 1)));
+  int16_t* del = bp<int16_t>(c, B_SELL_DEL);
+  k_sell_delta<<<waves_grid(c, (long long)nslices * 32, 256, 8), 256, 0, c->stream>>>(sidx, slots, n, nslices, off,
+                                                                                      del, maxdelta);
+  DCU_LAUNCHED(c, "k_sell_delta");
   DCU_TRY(ensure(c, B_SELL_KD, sizeof(int) * ((size_t)nslices + (size_t)(slots / 32) + 1)));
   int* su = bp<int>(c, B_SELL_KD);
   int* kd = su + nslices;
@@ -681,15 +715,24 @@ int sell_fill_from_csr(Ctx* c, int n, int nnz, const int* rptr, const int* rcol,
   int* wide = bp<int>(c, B_SELL_WIDE);
   DCU_TRY(ensure(c, B_SELL_KD8, (sizeof(int) + sizeof(int16_t)) * kNarrow * (size_t)nslices));
   int* kd8 = bp<int>(c, B_SELL_KD8);
-  int16_t* kd8h = plan->delta16 ? reinterpret_cast<int16_t*>(kd8 + kNarrow * (size_t)nslices) : nullptr;
+  int16_t* kd8h = reinterpret_cast<int16_t*>(kd8 + kNarrow * (size_t)nslices);
   DCU_CUDA(c, cudaMemsetAsync(wide, 0, sizeof(int), c->stream));
   k_sell_desc<<<waves_grid(c, (long long)nslices * 32, 256, 8), 256, 0, c->stream>>>(sidx, n, nslices, off, kd, su,
                                                                                        pst + 1, rptr, wide,
                                                                                        c->wide_prepass ? 1 : 0, kd8, kd8h);
   DCU_LAUNCHED(c, "k_sell_desc");
   DCU_CUDA(c, cudaMemcpyAsync(c->pinned, wide, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  DCU_CUDA(c, cudaMemcpyAsync(reinterpret_cast<int*>(c->pinned) + 1, maxdelta, sizeof(int), cudaMemcpyDeviceToHost,
+                              c->stream));
+  if (check)
+    DCU_CUDA(c, cudaMemcpyAsync(reinterpret_cast<int*>(c->pinned) + 2, check, sizeof(int), cudaMemcpyDeviceToHost,
+                                c->stream));
   DCU_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (check_out) *check_out = check ? reinterpret_cast<int*>(c->pinned)[2] : 0;
   plan->nwide = *reinterpret_cast<int*>(c->pinned);
+  plan->delta16 = reinterpret_cast<int*>(c->pinned)[1] < 32768;
+  plan->del = plan->delta16 ? del : nullptr;
+  if (!plan->delta16) kd8h = nullptr;
   c->plan_wide = plan->nwide;
   plan->wide = wide + 1;
   plan->rptr = rptr;
