@@ -36,7 +36,7 @@ namespace {
 
 constexpr int BI_BLOCK = 256;
 constexpr int BI_WARPS = BI_BLOCK / 32;
-constexpr int CHUNK_ITERS = 8;  // iterations per graph launch
+constexpr int CHUNK_ITERS = 4;  // iterations per graph launch (4 measured faster than 2 and 8)
 
 enum { ST_RUN = -1 };
 
