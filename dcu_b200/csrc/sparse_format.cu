@@ -265,15 +265,34 @@ __global__ void k_sell_width(const int* __restrict__ rptr, int n, int nslices, i
 // Otherwise the compact layout: row entries in order, padding at the end.
 // Rows keep their column order either way; padding slots have perm = -1 and,
 // in the compact layout or where row + offset leaves [0, n), column = row.
-__global__ void k_sell_fill(const int* __restrict__ rptr, const int* __restrict__ rcol, const int* __restrict__ rperm,
-                            int n, int nslices, const long long* __restrict__ off, int* __restrict__ sidx,
-                            int* __restrict__ sperm, int* __restrict__ maxdelta) {
+//
+// The same pass describes each slot it writes, from the column in hand:
+//   del[q] = column - row as int16 (read only when maxdelta < 32768);
+//   kd[off[s] / 32 + k] = (d << 1) | 1 when every row of the slice below n
+//     has its k-th slot at one offset d, else 0;
+//   su[s] bit 0 when every k has one offset (the SpMV then reads no index),
+//     bit 1 (narrow) when in addition the slice is at most kNarrow wide, with
+//     its width in bits 3-6 and kd8[kNarrow s + k] = d (kd8h as int16), bit 2
+//     (wide) for a full slice wider than kWideSlice made so by at most
+//     kWideRows long rows, listed in wide (wide[0] counts);
+//   *uslots += the slots of the uniform slices (one atomic per block).
+__global__ void k_sell_layout(const int* __restrict__ rptr, const int* __restrict__ rcol,
+                              const int* __restrict__ rperm, int n, int nslices, const long long* __restrict__ off,
+                              int* __restrict__ sidx, int* __restrict__ sperm, int* __restrict__ maxdelta,
+                              int16_t* __restrict__ del, int* __restrict__ kd, int* __restrict__ su,
+                              unsigned long long* __restrict__ uslots, int* __restrict__ wide, int allow_wide,
+                              int* __restrict__ kd8, int16_t* __restrict__ kd8h) {
+  __shared__ unsigned long long blk_uslots;
+  if (threadIdx.x == 0) blk_uslots = 0ull;
+  __syncthreads();
+  unsigned long long my_uslots = 0ull;  // lane 0 of each warp: uniform slots of its slices
   const int rows_total = nslices * 32;
   int local_max = 0;
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows_total; r += gridDim.x * blockDim.x) {
     const int s = r >> 5, lane = r & 31;
-    const long long base = off[s] + lane;
-    const int w = (int)((off[s + 1] - off[s]) >> 5);
+    const long long o0 = off[s];
+    const long long base = o0 + lane;
+    const int w = (int)((off[s + 1] - o0) >> 5);
     int rs = 0, len = 0;
     if (r < n) {
       rs = rptr[r];
@@ -281,85 +300,11 @@ __global__ void k_sell_fill(const int* __restrict__ rptr, const int* __restrict_
     }
     const int self = (r < n) ? r : 0;
     for (int j = 0; j < len; ++j) local_max = max(local_max, abs(rcol[rs + j] - self));
-    int i = 0;
-    for (int k = 0; k < w; ++k) {
-      const int cand = (i < len) ? rcol[rs + i] - r : INT_MAX;
-      const int m = __reduce_min_sync(0xffffffffu, cand);
-      const long long q = base + 32ll * k;
-      if (i < len && cand == m) {
-        sidx[q] = rcol[rs + i];
-        sperm[q] = rperm[rs + i];
-        ++i;
-      } else {
-        int c = self;
-        if (r < n && m != INT_MAX && (long long)r + m >= 0 && (long long)r + m < n) c = r + m;
-        sidx[q] = c;
-        sperm[q] = -1;
-      }
-    }
-    if (!__all_sync(0xffffffffu, i == len)) {
-      for (int k = 0; k < w; ++k) {
-        const long long q = base + 32ll * k;
-        if (k < len) {
-          sidx[q] = rcol[rs + k];
-          sperm[q] = rperm[rs + k];
-        } else {
-          sidx[q] = self;
-          sperm[q] = -1;
-        }
-      }
-    }
-  }
-#pragma unroll
-  for (int d = 16; d > 0; d >>= 1) local_max = max(local_max, __shfl_xor_sync(0xffffffffu, local_max, d));
-  if ((threadIdx.x & 31) == 0) atomicMax(maxdelta, local_max);
-}
-
-__global__ void k_sell_delta(const int* __restrict__ sidx, long long slots, int n, int nslices,
-                             const long long* __restrict__ off, int16_t* __restrict__ del,
-                             const int* __restrict__ maxdelta) {
-  // deltas of 16 bits only when every |col - row| < 32768 (k_sell_fill's
-  // maximum); otherwise every block returns at once
-  if (*maxdelta >= 32768) return;
-  // slot q belongs to row 32 s + ((q - off[s]) mod 32); recover s by walking
-  // per row instead: one thread per (row, k) over whole slices.
-  int rows_total = nslices * 32;
-  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows_total; r += gridDim.x * blockDim.x) {
-    int s = r >> 5, lane = r & 31;
-    long long base = off[s] + lane;
-    int w = (int)((off[s + 1] - off[s]) >> 5);
-    int self = (r < n) ? r : 0;
-    for (int k = 0; k < w; ++k) {
-      long long q = base + 32ll * k;
-      del[q] = (int16_t)(sidx[q] - self);
-    }
-  }
-}
-
-// One warp per slice (rows 32 s .. 32 s + 31 on the lanes): for every k,
-// whether all of the slice's rows below n have their k-th slot at the same
-// offset d = column - row.  Rows past n (last slice) never run and do not
-// count.  Writes kd[off[s] / 32 + k] = (d << 1) | 1, or 0, and su[s] = 1 when
-// every k of the slice has one offset (the SpMV then reads no index at all);
-// for such a slice at most kNarrow wide also the narrow flag, its width and
-// kd8[kNarrow s + k] = d (the SellPlan::su bits).
-__global__ void k_sell_desc(const int* __restrict__ sidx, int n, int nslices, const long long* __restrict__ off,
-                            int* __restrict__ kd, int* __restrict__ su, unsigned long long* __restrict__ uslots,
-                            const int* __restrict__ rptr, int* __restrict__ wide, int allow_wide,
-                            int* __restrict__ kd8, int16_t* __restrict__ kd8h) {
-  __shared__ unsigned long long blk_uslots;
-  if (threadIdx.x == 0) blk_uslots = 0ull;
-  __syncthreads();
-  unsigned long long my_uslots = 0ull;  // lane 0 of each warp: uniform slots of its slices
-  const int rows_total = nslices * 32;
-  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows_total; r += gridDim.x * blockDim.x) {
-    const int s = r >> 5, lane = r & 31;
-    const long long o0 = off[s];
-    const int w = (int)((off[s + 1] - o0) >> 5);
     bool all = true;
     int my_d = 0;  // lane k < kNarrow: offset of entry position k
-    // position k of the slice (w is the same for the whole warp)
-    auto position = [&](int k, int col) {
+    // slot k of this row holds column col: its delta and the slice's offset check
+    auto note = [&](int k, long long q, int col) {
+      del[q] = (int16_t)(col - self);
       const int d = col - r;
       const int d0 = __shfl_sync(0xffffffffu, d, 0);  // row 32 s < n always
       const bool same = __all_sync(0xffffffffu, r >= n || d == d0);
@@ -367,22 +312,48 @@ __global__ void k_sell_desc(const int* __restrict__ sidx, int n, int nslices, co
       if (lane == 0) kd[(o0 >> 5) + k] = same ? (int)(((unsigned)d0 << 1) | 1u) : 0;
       if (lane == k) my_d = d0;
     };
-    // the first kNarrow positions' columns are loaded together
-    int pre[kNarrow];
-#pragma unroll
-    for (int k = 0; k < kNarrow; ++k) pre[k] = (k < w) ? sidx[o0 + 32ll * k + lane] : 0;
-#pragma unroll
-    for (int k = 0; k < kNarrow; ++k)
-      if (k < w) position(k, pre[k]);
-    for (int k = kNarrow; k < w; ++k) position(k, sidx[o0 + 32ll * k + lane]);
+    int i = 0;
+    for (int k = 0; k < w; ++k) {
+      const int cand = (i < len) ? rcol[rs + i] - r : INT_MAX;
+      const int m = __reduce_min_sync(0xffffffffu, cand);
+      const long long q = base + 32ll * k;
+      int col;
+      if (i < len && cand == m) {
+        col = rcol[rs + i];
+        sperm[q] = rperm[rs + i];
+        ++i;
+      } else {
+        col = self;
+        if (r < n && m != INT_MAX && (long long)r + m >= 0 && (long long)r + m < n) col = r + m;
+        sperm[q] = -1;
+      }
+      sidx[q] = col;
+      note(k, q, col);
+    }
+    if (!__all_sync(0xffffffffu, i == len)) {
+      all = true;
+      my_d = 0;
+      for (int k = 0; k < w; ++k) {
+        const long long q = base + 32ll * k;
+        int col;
+        if (k < len) {
+          col = rcol[rs + k];
+          sperm[q] = rperm[rs + k];
+        } else {
+          col = self;
+          sperm[q] = -1;
+        }
+        sidx[q] = col;
+        note(k, q, col);
+      }
+    }
     const bool narrow = all && w > 0 && w <= kNarrow;
     if (lane < kNarrow) {
       const int d = (narrow && lane < w) ? my_d : 0;
       kd8[(long long)s * kNarrow + lane] = d;
-      if (kd8h) kd8h[(long long)s * kNarrow + lane] = (int16_t)d;  // read only when every |d| < 32768
+      kd8h[(long long)s * kNarrow + lane] = (int16_t)d;  // read only when every |d| < 32768
     }
     // rows of the slice longer than kWideSlice
-    const int len = (r < n) ? rptr[r + 1] - rptr[r] : 0;
     const int nlong = __popc(__ballot_sync(0xffffffffu, len > kWideSlice));
     if (lane == 0) {
       int f = all ? 1 : 0;
@@ -390,14 +361,17 @@ __global__ void k_sell_desc(const int* __restrict__ sidx, int n, int nslices, co
       // a full slice made wide by a few long rows: listed for the solver's
       // pre-pass (wide[0] counts, wide[1 + i] = slice)
       if (allow_wide && w > kWideSlice && nlong <= kWideRows && 32 * s + 32 <= n) {
-        const int i = atomicAdd(wide, 1);
-        wide[1 + i] = s;
-        f |= 4 | (i << 3);
+        const int wi = atomicAdd(wide, 1);
+        wide[1 + wi] = s;
+        f |= 4 | (wi << 3);
       }
       su[s] = f;
       if (all && w > 0) my_uslots += 32ull * (unsigned long long)w;
     }
   }
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) local_max = max(local_max, __shfl_xor_sync(0xffffffffu, local_max, d));
+  if ((threadIdx.x & 31) == 0) atomicMax(maxdelta, local_max);
   // one atomic per block (the warps' loop trip counts differ: no barrier
   // inside the loop; lane 0 of each warp adds its total here)
   if ((threadIdx.x & 31) == 0 && my_uslots) atomicAdd(&blk_uslots, my_uslots);
@@ -693,17 +667,11 @@ int sell_fill_from_csr(Ctx* c, int n, int nnz, const int* rptr, const int* rcol,
   DCU_TRY(ensure(c, B_ROWCNT, sizeof(int) * (size_t)(n + 1)));
   int* maxdelta = bp<int>(c, B_ROWCNT);  // row counts are no longer needed
   DCU_CUDA(c, cudaMemsetAsync(maxdelta, 0, sizeof(int), c->stream));
-  k_sell_fill<<<waves_grid(c, (long long)nslices * 32, 256, 8), 256, 0, c->stream>>>(rptr, rcol, rperm, n, nslices, off,
-                                                                                     sidx, sperm, maxdelta);
-  DCU_LAUNCHED(c, "k_sell_fill");
-  // the 16-bit deltas and their offsets table are written unless the
-  // maximum |col - row| rules them out; the host reads that maximum with the
-  // wide-slice count at the end, one round trip for both
+  // the 16-bit deltas are written always and read only when the maximum
+  // |col - row| allows them; the host reads that maximum with the wide-slice
+  // count at the end, one round trip for both
   DCU_TRY(ensure(c, B_SELL_DEL, sizeof(int16_t) * (size_t)(slots > 0 ? slots : 1)));
   int16_t* del = bp<int16_t>(c, B_SELL_DEL);
-  k_sell_delta<<<waves_grid(c, (long long)nslices * 32, 256, 8), 256, 0, c->stream>>>(sidx, slots, n, nslices, off,
-                                                                                      del, maxdelta);
-  DCU_LAUNCHED(c, "k_sell_delta");
   DCU_TRY(ensure(c, B_SELL_KD, sizeof(int) * ((size_t)nslices + (size_t)(slots / 32) + 1)));
   int* su = bp<int>(c, B_SELL_KD);
   int* kd = su + nslices;
@@ -717,10 +685,10 @@ int sell_fill_from_csr(Ctx* c, int n, int nnz, const int* rptr, const int* rcol,
   int* kd8 = bp<int>(c, B_SELL_KD8);
   int16_t* kd8h = reinterpret_cast<int16_t*>(kd8 + kNarrow * (size_t)nslices);
   DCU_CUDA(c, cudaMemsetAsync(wide, 0, sizeof(int), c->stream));
-  k_sell_desc<<<waves_grid(c, (long long)nslices * 32, 256, 8), 256, 0, c->stream>>>(sidx, n, nslices, off, kd, su,
-                                                                                       pst + 1, rptr, wide,
-                                                                                       c->wide_prepass ? 1 : 0, kd8, kd8h);
-  DCU_LAUNCHED(c, "k_sell_desc");
+  k_sell_layout<<<waves_grid(c, (long long)nslices * 32, 256, 8), 256, 0, c->stream>>>(
+      rptr, rcol, rperm, n, nslices, off, sidx, sperm, maxdelta, del, kd, su, pst + 1, wide, c->wide_prepass ? 1 : 0,
+      kd8, kd8h);
+  DCU_LAUNCHED(c, "k_sell_layout");
   DCU_CUDA(c, cudaMemcpyAsync(c->pinned, wide, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   DCU_CUDA(c, cudaMemcpyAsync(reinterpret_cast<int*>(c->pinned) + 1, maxdelta, sizeof(int), cudaMemcpyDeviceToHost,
                               c->stream));
