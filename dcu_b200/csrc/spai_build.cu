@@ -28,6 +28,7 @@
 // for every schedule and grid size.
 #include <algorithm>
 #include <climits>
+#include <type_traits>
 #include <vector>
 
 #include "internal.cuh"
@@ -481,7 +482,8 @@ struct NeArgs {
   double tau;
 };
 
-__host__ __device__ constexpr int tri(int a, int b) { return a * NE_NJ - (a * (a - 1)) / 2 + (b - a); }
+template <int N>
+__host__ __device__ constexpr int tri_n(int a, int b) { return a * N - (a * (a - 1)) / 2 + (b - a); }
 
 template <typename T>
 __global__ void __launch_bounds__(NE_BLOCK) k_spai_ne(NeArgs a) {
@@ -492,7 +494,11 @@ __global__ void __launch_bounds__(NE_BLOCK) k_spai_ne(NeArgs a) {
   const int tid = threadIdx.x;
   int my_cols = 0, my_max_nj = 0;
 
-  auto process = [&](int k) {
+  // Column k with |J| <= NJ (NJ: the register tiles' size, a compile-time
+  // constant; padding positions hold zeros and the identity, which leave the
+  // others' values unchanged bit for bit).
+  auto process = [&](auto njc, int k) {
+    constexpr int NJ = decltype(njc)::value;
     const int cs = __ldg(a.ptr + k);
     const int nj = __ldg(a.ptr + k + 1) - cs;
     my_max_nj = max(my_max_nj, nj);
@@ -501,14 +507,14 @@ __global__ void __launch_bounds__(NE_BLOCK) k_spai_ne(NeArgs a) {
       ++my_cols;
       return;
     }
-    if (nj > NE_NJ) {
+    if (nj > NJ) {
       a.fb_list[atomicAdd(&a.stats[ST_FB_COUNT], 1)] = k;
       return;
     }
-    int base[NE_NJ], len[NE_NJ], cb[NE_NJ];
+    int base[NJ], len[NJ], cb[NJ];
     int cand = 0;
 #pragma unroll
-    for (int j = 0; j < NE_NJ; ++j) {
+    for (int j = 0; j < NJ; ++j) {
       base[j] = 0;
       len[j] = 0;
       if (j < nj) {
@@ -525,7 +531,7 @@ __global__ void __launch_bounds__(NE_BLOCK) k_spai_ne(NeArgs a) {
     }
     bool sorted = true;
 #pragma unroll
-    for (int j = 0; j < NE_NJ; ++j) {
+    for (int j = 0; j < NJ; ++j) {
       int prev = -1;
       for (int q = 0; q < len[j]; ++q) {
         const int r = __ldg(a.idx + base[j] + q);
@@ -536,11 +542,11 @@ __global__ void __launch_bounds__(NE_BLOCK) k_spai_ne(NeArgs a) {
       }
     }
     // G (upper triangle) and g = A(k, J)^T
-    T G[NE_NJ * (NE_NJ + 1) / 2], g[NE_NJ];
+    T G[NJ * (NJ + 1) / 2], g[NJ];
 #pragma unroll
-    for (int i = 0; i < NE_NJ * (NE_NJ + 1) / 2; ++i) G[i] = T(0);
+    for (int i = 0; i < NJ * (NJ + 1) / 2; ++i) G[i] = T(0);
 #pragma unroll
-    for (int j = 0; j < NE_NJ; ++j) g[j] = T(0);
+    for (int j = 0; j < NJ; ++j) g[j] = T(0);
     if (sorted) {
       // Rows ascending in every column: one K-way merge over the columns.
       // Each step takes the smallest row r left among the column heads,
@@ -548,20 +554,20 @@ __global__ void __launch_bounds__(NE_BLOCK) k_spai_ne(NeArgs a) {
       // and v to g when r = k.  Every G entry sums its products in ascending
       // row order, as a pairwise merge would; each entry is read once.  Each
       // step consumes at least one entry, so it runs at most cand times.
-      int pos[NE_NJ], head[NE_NJ];
+      int pos[NJ], head[NJ];
 #pragma unroll
-      for (int j = 0; j < NE_NJ; ++j) {
+      for (int j = 0; j < NJ; ++j) {
         pos[j] = cb[j];
         head[j] = (len[j] > 0) ? srow[cb[j] * NE_BLOCK + tid] : INT_MAX;
       }
       for (int step = 0; step < cand; ++step) {
         int m = head[0];
 #pragma unroll
-        for (int j = 1; j < NE_NJ; ++j) m = min(m, head[j]);
+        for (int j = 1; j < NJ; ++j) m = min(m, head[j]);
         if (m == INT_MAX) break;
-        T v[NE_NJ];
+        T v[NJ];
 #pragma unroll
-        for (int j = 0; j < NE_NJ; ++j) {
+        for (int j = 0; j < NJ; ++j) {
           v[j] = T(0);
           if (head[j] == m) {
             v[j] = sval[pos[j] * NE_BLOCK + tid];
@@ -571,60 +577,60 @@ __global__ void __launch_bounds__(NE_BLOCK) k_spai_ne(NeArgs a) {
         }
         if (m == k) {
 #pragma unroll
-          for (int j = 0; j < NE_NJ; ++j) g[j] += v[j];
+          for (int j = 0; j < NJ; ++j) g[j] += v[j];
         }
 #pragma unroll
-        for (int ja = 0; ja < NE_NJ; ++ja) {
+        for (int ja = 0; ja < NJ; ++ja) {
 #pragma unroll
-          for (int jb = ja; jb < NE_NJ; ++jb) G[tri(ja, jb)] += v[ja] * v[jb];
+          for (int jb = ja; jb < NJ; ++jb) G[tri_n<NJ>(ja, jb)] += v[ja] * v[jb];
         }
       }
     } else {
 #pragma unroll
-      for (int ja = 0; ja < NE_NJ; ++ja) {
+      for (int ja = 0; ja < NJ; ++ja) {
         for (int p = cb[ja]; p < cb[ja] + len[ja]; ++p) {
           const int r = srow[p * NE_BLOCK + tid];
           const T v = sval[p * NE_BLOCK + tid];
           if (r == k) g[ja] += v;
-          G[tri(ja, ja)] += v * v;
+          G[tri_n<NJ>(ja, ja)] += v * v;
         }
       }
 #pragma unroll
-      for (int ja = 0; ja < NE_NJ; ++ja) {
+      for (int ja = 0; ja < NJ; ++ja) {
         for (int p = cb[ja]; p < cb[ja] + len[ja]; ++p) {
           const int r = srow[p * NE_BLOCK + tid];
           const T v = sval[p * NE_BLOCK + tid];
 #pragma unroll
-          for (int jb = ja + 1; jb < NE_NJ; ++jb) {
+          for (int jb = ja + 1; jb < NJ; ++jb) {
             T acc = T(0);
             for (int q = cb[jb]; q < cb[jb] + len[jb]; ++q)
               if (srow[q * NE_BLOCK + tid] == r) acc += sval[q * NE_BLOCK + tid];
-            G[tri(ja, jb)] += v * acc;
+            G[tri_n<NJ>(ja, jb)] += v * acc;
           }
         }
       }
     }
     // pad to 8 x 8 with the identity, factor G = U^T U in place
 #pragma unroll
-    for (int j = 0; j < NE_NJ; ++j)
-      if (j >= nj) G[tri(j, j)] = T(1);
+    for (int j = 0; j < NJ; ++j)
+      if (j >= nj) G[tri_n<NJ>(j, j)] = T(1);
     bool ok = true;
 #pragma unroll
-    for (int j = 0; j < NE_NJ; ++j) {
-      const T gjj = G[tri(j, j)];
+    for (int j = 0; j < NJ; ++j) {
+      const T gjj = G[tri_n<NJ>(j, j)];
       T d = gjj;
 #pragma unroll
-      for (int p = 0; p < j; ++p) d -= G[tri(p, j)] * G[tri(p, j)];
+      for (int p = 0; p < j; ++p) d -= G[tri_n<NJ>(p, j)] * G[tri_n<NJ>(p, j)];
       if (!(d > (T)a.tau * gjj) || !isfinite((double)d)) ok = false;
       const T ujj = sqrt(d > T(0) ? d : T(1));
       const T inv = T(1) / ujj;
-      G[tri(j, j)] = ujj;
+      G[tri_n<NJ>(j, j)] = ujj;
 #pragma unroll
-      for (int i = j + 1; i < NE_NJ; ++i) {
-        T t = G[tri(j, i)];
+      for (int i = j + 1; i < NJ; ++i) {
+        T t = G[tri_n<NJ>(j, i)];
 #pragma unroll
-        for (int p = 0; p < j; ++p) t -= G[tri(p, j)] * G[tri(p, i)];
-        G[tri(j, i)] = t * inv;
+        for (int p = 0; p < j; ++p) t -= G[tri_n<NJ>(p, j)] * G[tri_n<NJ>(p, i)];
+        G[tri_n<NJ>(j, i)] = t * inv;
       }
     }
     if (!ok) {
@@ -632,24 +638,24 @@ __global__ void __launch_bounds__(NE_BLOCK) k_spai_ne(NeArgs a) {
       return;
     }
     // U^T y = g, U x = y
-    T y[NE_NJ];
+    T y[NJ];
 #pragma unroll
-    for (int j = 0; j < NE_NJ; ++j) {
+    for (int j = 0; j < NJ; ++j) {
       T t = g[j];
 #pragma unroll
-      for (int p = 0; p < j; ++p) t -= G[tri(p, j)] * y[p];
-      y[j] = t / G[tri(j, j)];
+      for (int p = 0; p < j; ++p) t -= G[tri_n<NJ>(p, j)] * y[p];
+      y[j] = t / G[tri_n<NJ>(j, j)];
     }
 #pragma unroll
-    for (int j = NE_NJ - 1; j >= 0; --j) {
+    for (int j = NJ - 1; j >= 0; --j) {
       T t = y[j];
 #pragma unroll
-      for (int p = j + 1; p < NE_NJ; ++p) t -= G[tri(j, p)] * y[p];
-      y[j] = t / G[tri(j, j)];
+      for (int p = j + 1; p < NJ; ++p) t -= G[tri_n<NJ>(j, p)] * y[p];
+      y[j] = t / G[tri_n<NJ>(j, j)];
     }
     double gx = 0.0;
 #pragma unroll
-    for (int j = 0; j < NE_NJ; ++j)
+    for (int j = 0; j < NJ; ++j)
       if (j < nj) {
         a.mval[cs + j] = (double)y[j];
         gx += (double)g[j] * (double)y[j];
@@ -659,10 +665,17 @@ __global__ void __launch_bounds__(NE_BLOCK) k_spai_ne(NeArgs a) {
     ++my_cols;
   };
 
+  // columns with |J| <= 7 (every column of a 2D or 3D stencil) on 7-wide
+  // register tiles, the rest on 8-wide ones
+  auto column = [&](int k) {
+    if (__ldg(a.ptr + k + 1) - __ldg(a.ptr + k) <= 7) process(std::integral_constant<int, 7>{}, k);
+    else process(std::integral_constant<int, NE_NJ>{}, k);
+  };
+
   if (a.schedule == DCU_SCHED_BALANCED_COLUMNS) {
     // balanced_columns: one sweep of the whole range by all threads (see
     // k_spai_small)
-    for (int k = a.col_start + blockIdx.x * NE_BLOCK + tid; k < a.col_end; k += gridDim.x * NE_BLOCK) process(k);
+    for (int k = a.col_start + blockIdx.x * NE_BLOCK + tid; k < a.col_end; k += gridDim.x * NE_BLOCK) column(k);
   } else {
     for (;;) {
       if (tid == 0) s_chunk = atomicAdd(&a.stats[ST_DYN_HEAD], 1);
@@ -670,7 +683,7 @@ __global__ void __launch_bounds__(NE_BLOCK) k_spai_ne(NeArgs a) {
       const int ch = s_chunk;
       __syncthreads();
       if (ch >= a.nchunks) break;
-      for (int k = a.chunks[ch] + tid; k < a.chunks[ch + 1]; k += NE_BLOCK) process(k);
+      for (int k = a.chunks[ch] + tid; k < a.chunks[ch + 1]; k += NE_BLOCK) column(k);
     }
   }
 #pragma unroll

@@ -43,16 +43,19 @@ __global__ void k_row_scatter(const int* __restrict__ ptr, const int* __restrict
 // by binary search.  One thread per column; flag bit 1 = a column is not
 // strictly ascending, bit 2 = some (r, c) has no (c, r).  Any flag sends the
 // conversion to the general count / scatter / sort path, which rewrites all
-// three outputs.
+// three outputs.  With copies = 0 only rperm is written (the caller reads
+// ptr and idx as the CSR arrays).
 __global__ void k_csr_symmetric(const int* __restrict__ ptr, const int* __restrict__ idx, int n,
                                 int* __restrict__ rptr, int* __restrict__ rcol, int* __restrict__ rperm,
-                                int* __restrict__ flag) {
+                                int* __restrict__ flag, int copies) {
   constexpr int kShort = 8;  // columns up to this long search their partners side by side
   int bad = 0;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
     const int s = ptr[c], e = ptr[c + 1];
-    rptr[c] = s;
-    if (c == n - 1) rptr[n] = e;
+    if (copies) {
+      rptr[c] = s;
+      if (c == n - 1) rptr[n] = e;
+    }
     if (e - s <= kShort) {
       // the entries' rows, their columns' ranges, then the binary searches
       // one step at a time for all entries: a few dependent loads per column
@@ -65,7 +68,7 @@ __global__ void k_csr_symmetric(const int* __restrict__ ptr, const int* __restri
 #pragma unroll
       for (int t = 0; t < kShort; ++t) {
         if (t < len) {
-          rcol[s + t] = r[t];
+          if (copies) rcol[s + t] = r[t];
           if (r[t] <= prev) bad |= 1;
           prev = r[t];
           lo[t] = ptr[r[t]];
@@ -102,7 +105,7 @@ __global__ void k_csr_symmetric(const int* __restrict__ ptr, const int* __restri
     int prev = -1;
     for (int k = s; k < e; ++k) {
       const int r = idx[k];
-      rcol[k] = r;
+      if (copies) rcol[k] = r;
       if (r <= prev) bad |= 1;
       prev = r;
       int lo = ptr[r], hi = ptr[r + 1] - 1, q = -1;
@@ -562,11 +565,12 @@ namespace {
 // 0 when the pattern was symmetric with ascending columns and the result
 // stands, else the general path must run.
 int csr_try_symmetric(Ctx* c, int n, const int* ptr, const int* idx, int* rptr, int* rcol, int* rperm,
-                      int** flag) {
+                      int** flag, bool copies) {
   DCU_TRY(ensure(c, B_LONGROWS, sizeof(int) * (size_t)(n + 2)));
   int* longcount = bp<int>(c, B_LONGROWS) + n;
   DCU_CUDA(c, cudaMemsetAsync(longcount, 0, 2 * sizeof(int), c->stream));
-  k_csr_symmetric<<<waves_grid(c, n, 256, 8), 256, 0, c->stream>>>(ptr, idx, n, rptr, rcol, rperm, longcount);
+  k_csr_symmetric<<<waves_grid(c, n, 256, 8), 256, 0, c->stream>>>(ptr, idx, n, rptr, rcol, rperm, longcount,
+                                                                     copies ? 1 : 0);
   DCU_LAUNCHED(c, "k_csr_symmetric");
   *flag = longcount;
   return DCU_OK;
@@ -616,7 +620,7 @@ int csr_general(Ctx* c, int n, int nnz, const int* ptr, const int* idx, int* rpt
 int csr_from_csc(Ctx* c, int n, int nnz, const int* ptr, const int* idx, int* rptr, int* rcol, int* rperm) {
   if (n > 0 && nnz > 0) {
     int* flag = nullptr;
-    DCU_TRY(csr_try_symmetric(c, n, ptr, idx, rptr, rcol, rperm, &flag));
+    DCU_TRY(csr_try_symmetric(c, n, ptr, idx, rptr, rcol, rperm, &flag, true));
     DCU_CUDA(c, cudaMemcpyAsync(c->pinned, flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     DCU_CUDA(c, cudaStreamSynchronize(c->stream));
     if (*(int*)c->pinned == 0) return DCU_OK;
@@ -636,11 +640,12 @@ int sell_plan(Ctx* c, int n, int nnz, const int* ptr, const int* idx, SellPlan* 
     // its verdict, which comes back with the layout's last round trip; a
     // pattern that is not symmetric (the speculative layout stays in bounds:
     // its row pointers, columns and slots are A's own) is laid out again
-    // from the general conversion
+    // from the general conversion.  A symmetric pattern's CSR row pointers
+    // and columns are A's CSC arrays themselves: the layout reads those.
     int* flag = nullptr;
-    DCU_TRY(csr_try_symmetric(c, n, ptr, idx, rptr, rcol, rperm, &flag));
+    DCU_TRY(csr_try_symmetric(c, n, ptr, idx, rptr, rcol, rperm, &flag, false));
     int bad = 0;
-    DCU_TRY(sell_fill_from_csr(c, n, nnz, rptr, rcol, rperm, plan, flag, &bad));
+    DCU_TRY(sell_fill_from_csr(c, n, nnz, ptr, idx, rperm, plan, flag, &bad));
     if (bad == 0) return DCU_OK;
   }
   DCU_TRY(csr_general(c, n, nnz, ptr, idx, rptr, rcol, rperm));
