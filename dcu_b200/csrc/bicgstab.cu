@@ -335,7 +335,15 @@ __device__ __forceinline__ double m_row(const BiArgs<MT, IT, VT>& a, int r, F xf
 
 // Kernels K1..K5 are launched with programmatic dependent launch: their blocks
 // may start while the previous kernel drains, and wait here for its results.
+// Every kernel of the iteration starts here.  It first lets the next kernel
+// in the stream (launched with programmatic dependent launch) be scheduled:
+// that launch happens once every block of this grid has passed this point,
+// so its blocks only take slots this grid no longer needs, and they become
+// resident while this grid finishes instead of after it.  Then it waits for
+// the previous kernel to complete with its memory visible (the wait covers
+// completion, not the trigger), and reads the stop flag.
 __device__ __forceinline__ bool finished(const Scal* S) {
+  cudaTriggerProgrammaticLaunchCompletion();
   cudaGridDependencySynchronize();
   return *(volatile const int*)&S->done != 0;
 }
