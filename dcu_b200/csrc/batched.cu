@@ -231,7 +231,32 @@ __device__ __forceinline__ const double* system_reduce(double (&v)[ND][vals_per_
   return totals;
 }
 
-__device__ __forceinline__ bool g_finished(const BGlobal* g) { return *(volatile const int*)&g->done != 0; }
+// Every kernel of the batched iteration starts here: it lets the next kernel
+// (programmatic dependent launch) be scheduled once all its blocks have
+// passed this point, waits for the previous kernel to complete with its
+// memory visible, then reads the batch's stop flag.
+__device__ __forceinline__ bool g_finished(const BGlobal* g) {
+  cudaTriggerProgrammaticLaunchCompletion();
+  cudaGridDependencySynchronize();
+  return *(volatile const int*)&g->done != 0;
+}
+
+// Launch with programmatic dependent launch (inside the captured graph: a
+// programmatic edge from the previous kernel).
+template <typename K, typename A>
+cudaError_t launch_pdl_b(K kernel, int grid, int block, cudaStream_t st, const A& args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, args);
+}
 
 // A system whose every pair stopped is skipped by all its tiles (nothing reads
 // its vectors or partials any more).
@@ -638,15 +663,20 @@ int run_batch(Ctx* c, int nsys, const int* sys_off_d, const SellPlan& plan, cons
   if (!ge) {
     cudaGraph_t gr = nullptr;
     DCU_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    for (int i = 0; i < BCHUNK; ++i) {
-      kb_py<R><<<ntiles, BT, 0, c->stream>>>(a);
-      kb_ay<R><<<ntiles, BT, 0, c->stream>>>(a);
-      kb_sz<R><<<ntiles, BT, 0, c->stream>>>(a);
-      kb_az<R><<<ntiles, BT, 0, c->stream>>>(a);
-      kb_xr<R><<<ntiles, BT, 0, c->stream>>>(a);
-      kb_step<R><<<1, 1, 0, c->stream>>>(a);
+    cudaError_t le = cudaSuccess;
+    for (int i = 0; i < BCHUNK && le == cudaSuccess; ++i) {
+      le = launch_pdl_b(kb_py<R>, ntiles, BT, c->stream, a);
+      if (le == cudaSuccess) le = launch_pdl_b(kb_ay<R>, ntiles, BT, c->stream, a);
+      if (le == cudaSuccess) le = launch_pdl_b(kb_sz<R>, ntiles, BT, c->stream, a);
+      if (le == cudaSuccess) le = launch_pdl_b(kb_az<R>, ntiles, BT, c->stream, a);
+      if (le == cudaSuccess) le = launch_pdl_b(kb_xr<R>, ntiles, BT, c->stream, a);
+      if (le == cudaSuccess) le = launch_pdl_b(kb_step<R>, 1, 1, c->stream, a);
     }
     cudaError_t e = cudaStreamEndCapture(c->stream, &gr);
+    if (le != cudaSuccess) {
+      if (gr) cudaGraphDestroy(gr);
+      return cuda_fail(c, le, "cudaLaunchKernelEx (capture)", __FILE__, __LINE__);
+    }
     if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture", __FILE__, __LINE__);
     GraphSlot ne;
     ne.key = key;
